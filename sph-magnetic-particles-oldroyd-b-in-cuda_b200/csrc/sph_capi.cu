@@ -1,0 +1,922 @@
+// sph_capi.cu -- the C ABI (include/sph_capi.h): context lifetime, device memory, the
+// order of the step phases (the reference's main.cu:358-467 and class_system methods),
+// CUDA-graph replay of whole steps, and state access in original particle order.
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cmath>
+#include <cstdio>
+#include <cstring>
+#include <string>
+#include <vector>
+
+#include "sph_internal.h"
+
+using namespace sph;
+
+struct sph_ctx {
+  int device = 0, prec = SPH_PREC_FP64, dim = 3, nboxes = 0, use_graph = 1;
+  std::vector<HostBox> boxes;
+  Dev d{};
+  cudaStream_t stream = nullptr;
+  std::vector<void*> allocs;
+  int key_bits = 1;
+  SortScratch sort{};
+  double* ke_partial = nullptr;
+  double* scratch = nullptr;  // Ntot doubles for field transfers
+  int* iscratch = nullptr;    // Ntot ints
+  std::string err;
+  long long launches = 0;
+  bool initial_done = false;
+  bool in_step = false;      // between vv_step1 and vv_step2
+  bool forces_live = false;  // forces computed and not yet consumed by a half-kick
+  bool pos_dirty = true;     // positions changed since the last neighbour search
+  bool gradv_valid = false;
+  long long host_step = 0;
+  int parity = 0;            // which of the double-buffered state arrays is current
+  cudaGraphExec_t graph[2] = {nullptr, nullptr};
+  long long graph_kernels = 0;
+  cudaEvent_t ev0 = nullptr, ev1 = nullptr;
+  bool events_recorded = false;  // ev0/ev1 bracket the last sph_step
+  double last_ms = 0.0;
+  int max_coll = 0;
+  int cap_grown = 0;
+};
+
+namespace {
+
+sph_status fail(sph_ctx* c, sph_status s, const std::string& m) {
+  if (c) c->err = m;
+  return s;
+}
+
+sph_status cuda_fail(sph_ctx* c, const char* where) {
+  cudaError_t e = cudaGetLastError();
+  if (e == cudaSuccess && last_launch_error() != 0) e = (cudaError_t)last_launch_error();
+  last_launch_error() = 0;
+  return fail(c, SPH_ERR_CUDA, std::string(where) + ": " + cudaGetErrorString(e));
+}
+
+template <typename T>
+bool dalloc(sph_ctx* c, T** p, size_t n) {
+  void* q = nullptr;
+  if (cudaMalloc(&q, std::max<size_t>(n, 1) * sizeof(T)) != cudaSuccess) return false;
+  cudaMemsetAsync(q, 0, std::max<size_t>(n, 1) * sizeof(T), c->stream);
+  c->allocs.push_back(q);
+  *p = static_cast<T*>(q);
+  return true;
+}
+
+Launch launcher(sph_ctx* c) {
+  Launch L;
+  L.d = c->d;
+  L.prec = c->prec;
+  L.stream = c->stream;
+  L.launches = &c->launches;
+  return L;
+}
+
+int bits_for(int n) {
+  int b = 1;
+  while ((1 << b) < n) ++b;
+  return b;
+}
+
+void swap_state(sph_ctx* c, bool with_forces) {
+  std::swap(c->d.pos, c->d.pos_b);
+  std::swap(c->d.vel, c->d.vel_b);
+  std::swap(c->d.conf, c->d.conf_b);
+  std::swap(c->d.tinfo, c->d.tinfo_b);
+  std::swap(c->d.gid, c->d.gid_b);
+  if (with_forces) {
+    std::swap(c->d.f, c->d.f_b);
+    std::swap(c->d.dcdt, c->d.dcdt_b);
+  }
+  c->parity ^= 1;
+}
+
+int derived_capacity(const std::vector<HostBox>& boxes, int dim) {
+  double worst = 0;
+  for (const HostBox& hb : boxes) {
+    const sph_input& in = hb.in;
+    double vol = 1.0;
+    int Ny = in.N[1];
+    double dx0 = in.L[0] / in.N[0], dx1 = in.L[1] / Ny;
+    vol = dx0 * dx1;
+    if (dim == 3) vol *= in.L[2] / in.N[2];
+    const double rc = hb.p.rcut;
+    double ball = dim == 3 ? 4.0 / 3.0 * M_PI * rc * rc * rc : M_PI * rc * rc;
+    worst = std::max(worst, ball / vol + 1.0);
+  }
+  int cap = (int)std::ceil(1.5 * worst + 32.0);
+  return (cap + 7) / 8 * 8;
+}
+
+// Reads and clears the device error flags.  Blocks on the stream.
+sph_status check_device(sph_ctx* c) {
+  unsigned st = 0;
+  int info[2] = {0, 0};
+  if (cudaMemcpyAsync(&st, c->d.status, sizeof(unsigned), cudaMemcpyDeviceToHost, c->stream) !=
+          cudaSuccess ||
+      cudaMemcpyAsync(info, c->d.err_info, 2 * sizeof(int), cudaMemcpyDeviceToHost, c->stream) !=
+          cudaSuccess ||
+      cudaStreamSynchronize(c->stream) != cudaSuccess)
+    return cuda_fail(c, "device status");
+  if (st == 0) return SPH_OK;
+  cudaMemsetAsync(c->d.status, 0, sizeof(unsigned), c->stream);
+  if (st & kStatNaN)
+    return fail(c, SPH_ERR_NAN, "non-finite particle position (global id " +
+                                    std::to_string(info[0]) + ")");
+  if (st & kStatCellRange)
+    return fail(c, SPH_ERR_CELL_RANGE, "particle hashed outside the cell grid (global id " +
+                                           std::to_string(info[0]) + ")");
+  if (st & kStatCapacity)
+    return fail(c, SPH_ERR_CAPACITY, "neighbour list capacity " + std::to_string(c->d.cap) +
+                                         " exceeded (" + std::to_string(info[1]) + " needed)");
+  return SPH_OK;
+}
+
+void drop_graphs(sph_ctx* c) {
+  for (auto& g : c->graph)
+    if (g) {
+      cudaGraphExecDestroy(g);
+      g = nullptr;
+    }
+}
+
+sph_status grow_capacity(sph_ctx* c, int needed) {
+  int cap = std::max(needed + needed / 4 + 8, c->d.cap + 32);
+  cap = (cap + 7) / 8 * 8;
+  int* nbr = nullptr;
+  if (cudaMalloc(&nbr, (size_t)cap * c->d.Npad * sizeof(int)) != cudaSuccess)
+    return fail(c, SPH_ERR_NOMEM, "cannot grow neighbour lists");
+  auto it = std::find(c->allocs.begin(), c->allocs.end(), (void*)c->d.nbr);
+  if (it != c->allocs.end()) {
+    cudaFree(*it);
+    *it = nbr;
+  }
+  c->d.nbr = nbr;
+  c->d.cap = cap;
+  c->cap_grown++;
+  drop_graphs(c);
+  return SPH_OK;
+}
+
+// ---- phases (all asynchronous) ----
+int ph_search(sph_ctx* c) {
+  Launch L = launcher(c);
+  const bool permute = c->forces_live;
+  if (launch_hash(L) || launch_sort(L, c->key_bits, c->sort) || launch_reorder(L, permute))
+    return 1;
+  swap_state(c, permute);
+  L = launcher(c);
+  if (launch_build_lists_dim(L, c->dim)) return 1;
+  if (c->d.ncoll > 0 && launch_colloid_cells_n(L, c->nboxes, c->max_coll)) return 1;
+  c->pos_dirty = false;
+  return 0;
+}
+
+int ph_forces(sph_ctx* c) {
+  Launch L = launcher(c);
+  L.d.gradv = nullptr;  // the fused pass keeps the gradient in registers
+  bool ext = false;
+  for (const HostBox& hb : c->boxes) ext = ext || hb.p.ext_force_type != 0;
+  if (launch_density_dim(L, c->dim)) return 1;
+  if (launch_pairs_dim(L, c->dim, kPairFused, ext ? 1 : 0)) return 1;
+  if (launch_wall_forces(L)) return 1;
+  bool pairs = false;
+  for (const HostBox& hb : c->boxes) pairs = pairs || hb.p.N_colloids >= 2;
+  if (launch_colloid_forces(L, pairs ? 1 : 0)) return 1;
+  c->forces_live = true;
+  c->gradv_valid = false;
+  return 0;
+}
+
+int ph_vv1(sph_ctx* c) {
+  Launch L = launcher(c);
+  if (launch_vv1_colloids(L) || launch_vv1_particles(L)) return 1;
+  c->forces_live = false;
+  c->pos_dirty = true;
+  return 0;
+}
+
+int ph_vv2(sph_ctx* c) {
+  Launch L = launcher(c);
+  if (launch_vv2(L) || launch_count_step(L)) return 1;
+  return 0;
+}
+
+// One full step: VV1, search, m(t), forces, VV2 (main.cu:358-432)
+int ph_step(sph_ctx* c) {
+  if (ph_vv1(c) || ph_search(c)) return 1;
+  if (launch_advance_time(launcher(c), 0)) return 1;
+  if (ph_forces(c) || ph_vv2(c)) return 1;
+  c->forces_live = true;
+  return 0;
+}
+
+sph_status upload_moment(sph_ctx* c, const double* m) {
+  std::vector<double> mm(3 * (size_t)c->nboxes);
+  for (int b = 0; b < c->nboxes; ++b)
+    for (int q = 0; q < 3; ++q) mm[3 * b + q] = m[q];
+  if (cudaMemcpyAsync(c->d.mag, mm.data(), mm.size() * sizeof(double), cudaMemcpyHostToDevice,
+                      c->stream) != cudaSuccess)
+    return cuda_fail(c, "magnetic moment upload");
+  cudaStreamSynchronize(c->stream);
+  return SPH_OK;
+}
+
+// Host-computed moment at the current time of every box (exactly as main.cu computes it).
+sph_status host_moment(sph_ctx* c, long long step) {
+  std::vector<double> mm(3 * (size_t)c->nboxes);
+  for (int b = 0; b < c->nboxes; ++b) {
+    const BoxParams& p = c->boxes[b].p;
+    const double ang = p.omega_magnet * (p.t0 + p.dt * (double)step);
+    mm[3 * b] = std::cos(ang);
+    mm[3 * b + 1] = std::sin(ang);
+    mm[3 * b + 2] = 0.0;
+  }
+  if (cudaMemcpyAsync(c->d.mag, mm.data(), mm.size() * sizeof(double), cudaMemcpyHostToDevice,
+                      c->stream) != cudaSuccess)
+    return cuda_fail(c, "magnetic moment upload");
+  cudaStreamSynchronize(c->stream);
+  return SPH_OK;
+}
+
+sph_status search_checked(sph_ctx* c) {
+  if (ph_search(c)) return cuda_fail(c, "neighbours_search");
+  sph_status s = check_device(c);
+  if (s == SPH_ERR_CAPACITY) {
+    int info[2];
+    cudaMemcpy(info, c->d.err_info, sizeof(info), cudaMemcpyDeviceToHost);
+    s = grow_capacity(c, info[1]);
+    if (s != SPH_OK) return s;
+    cudaMemsetAsync(c->d.err_info + 1, 0, sizeof(int), c->stream);
+    if (launch_build_lists_dim(launcher(c), c->dim)) return cuda_fail(c, "rebuild lists");
+    s = check_device(c);
+  }
+  return s;
+}
+
+sph_status ensure_lists(sph_ctx* c) {
+  if (!c->pos_dirty) return SPH_OK;
+  return search_checked(c);
+}
+
+sph_status do_initial(sph_ctx* c) {
+  sph_status s = host_moment(c, 0);
+  if (s != SPH_OK) return s;
+  s = search_checked(c);
+  if (s != SPH_OK) return s;
+  if (ph_forces(c)) return cuda_fail(c, "initial forces");
+  s = check_device(c);
+  if (s != SPH_OK) return s;
+  c->initial_done = true;
+  return SPH_OK;
+}
+
+sph_status capture_graphs(sph_ctx* c) {
+  drop_graphs(c);
+  for (int k = 0; k < 2; ++k) {
+    cudaGraph_t g = nullptr;
+    long long before = c->launches;
+    if (cudaStreamBeginCapture(c->stream, cudaStreamCaptureModeThreadLocal) != cudaSuccess)
+      return cuda_fail(c, "begin capture");
+    const bool live = c->forces_live, dirty = c->pos_dirty;
+    int bad = ph_step(c);
+    c->forces_live = live;
+    c->pos_dirty = dirty;
+    cudaError_t e = cudaStreamEndCapture(c->stream, &g);
+    if (bad || e != cudaSuccess) {
+      if (g) cudaGraphDestroy(g);
+      return fail(c, SPH_ERR_CUDA, std::string("graph capture failed: ") + cudaGetErrorString(e));
+    }
+    // the captured step flipped the buffer parity; graph[k] starts from parity k
+    e = cudaGraphInstantiate(&c->graph[c->parity ^ 1], g, 0);
+    cudaGraphDestroy(g);
+    if (e != cudaSuccess) return fail(c, SPH_ERR_CUDA, "graph instantiate failed");
+    c->graph_kernels = c->launches - before;
+    c->launches = before;
+  }
+  return SPH_OK;
+}
+
+void free_ctx(sph_ctx* c) {
+  if (!c) return;
+  drop_graphs(c);
+  for (void* p : c->allocs) cudaFree(p);
+  if (c->ev0) cudaEventDestroy(c->ev0);
+  if (c->ev1) cudaEventDestroy(c->ev1);
+  if (c->stream) cudaStreamDestroy(c->stream);
+  delete c;
+}
+
+}  // namespace
+
+// ======================================================================================
+extern "C" {
+
+const char* sph_status_string(sph_status s) {
+  switch (s) {
+    case SPH_OK: return "ok";
+    case SPH_ERR_BAD_INPUT: return "bad input";
+    case SPH_ERR_CUDA: return "cuda error";
+    case SPH_ERR_CELL_RANGE: return "particle outside the cell grid";
+    case SPH_ERR_NAN: return "non-finite position";
+    case SPH_ERR_TIMEOUT: return "timeout";
+    case SPH_ERR_STATE: return "invalid state or argument";
+    case SPH_ERR_NOMEM: return "out of memory";
+    case SPH_ERR_CAPACITY: return "neighbour list capacity exceeded";
+    case SPH_ERR_IO: return "i/o error";
+  }
+  return "unknown status";
+}
+
+const char* sph_last_error(const sph_ctx* ctx) { return ctx ? ctx->err.c_str() : "null context"; }
+
+sph_status sph_read_input(const char* path, sph_input* in, double* coll_buf, int coll_cap,
+                          char* msg, size_t msg_cap) {
+  if (!path || !in) return SPH_ERR_STATE;
+  std::vector<double> coll;
+  std::string m;
+  sph_status s = parse_input_file(path, in, &coll, &m);
+  if (s == SPH_OK && in->N_colloids > 0) {
+    if (!coll_buf || coll_cap < in->N_colloids) {
+      s = SPH_ERR_STATE;
+      m = "colloid buffer too small";
+    } else {
+      std::memcpy(coll_buf, coll.data(), coll.size() * sizeof(double));
+      in->coll_xyz = coll_buf;
+    }
+  } else if (s == SPH_OK) {
+    in->coll_xyz = nullptr;
+  }
+  if (msg && msg_cap) {
+    std::strncpy(msg, m.c_str(), msg_cap - 1);
+    msg[msg_cap - 1] = 0;
+  }
+  return s;
+}
+
+sph_status sph_create_ensemble(int nboxes, const sph_input* inputs,
+                               const char* const* particles_paths, const sph_options* opt,
+                               sph_ctx** out) {
+  if (!out || !inputs || nboxes <= 0) return SPH_ERR_STATE;
+  *out = nullptr;
+  sph_ctx* c = new sph_ctx();
+  sph_options o{};
+  o.precision = SPH_PREC_FP64;
+  o.use_graph = 1;
+  if (opt) o = *opt;
+  c->prec = o.precision == SPH_PREC_MIXED ? SPH_PREC_MIXED : SPH_PREC_FP64;
+  c->device = o.device;
+  c->use_graph = o.use_graph;
+  c->nboxes = nboxes;
+  c->boxes.resize(nboxes);
+  static thread_local std::string create_err;
+  for (int b = 0; b < nboxes; ++b) {
+    std::string m;
+    sph_status s = build_box(inputs[b], particles_paths ? particles_paths[b] : nullptr,
+                             &c->boxes[b], &m);
+    if (s != SPH_OK) {
+      fprintf(stderr, "sph_create: box %d: %s\n", b, m.c_str());
+      delete c;
+      return s;
+    }
+  }
+  c->dim = c->boxes[0].p.dim;
+  for (const HostBox& hb : c->boxes)
+    if (hb.p.dim != c->dim) {
+      fprintf(stderr, "sph_create: all boxes of a context must have the same dim\n");
+      delete c;
+      return SPH_ERR_BAD_INPUT;
+    }
+  int ndev = 0;
+  if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev <= c->device ||
+      cudaSetDevice(c->device) != cudaSuccess) {
+    fprintf(stderr, "sph_create: no usable CUDA device\n");
+    delete c;
+    return SPH_ERR_CUDA;
+  }
+  if (cudaStreamCreateWithFlags(&c->stream, cudaStreamNonBlocking) != cudaSuccess) {
+    delete c;
+    return SPH_ERR_CUDA;
+  }
+  cudaEventCreate(&c->ev0);
+  cudaEventCreate(&c->ev1);
+  // ---- offsets ----
+  int Ntot = 0, Ctot = 0, ncoll = 0, nwall = 0, ncc = 0, nlist = 0, nwl = 0;
+  for (HostBox& hb : c->boxes) {
+    BoxParams& p = hb.p;
+    p.slot0 = Ntot;
+    p.cell0 = Ctot;
+    p.coll0 = ncoll;
+    p.wall_seg0 = nwall;
+    p.ccell0 = ncc;
+    p.list_cut2 = p.rcutsq * (1.0 + 1.0e-4);
+    Ntot += p.N;
+    Ctot += p.Ntotal_cells;
+    ncoll += p.N_colloids;
+    nwall += p.wall ? 2 : 0;
+    ncc += p.N_colloids > 0 ? p.Ntotal_cells_colloids : 0;
+    nlist += (int)hb.colloids_list.size();
+    nwl += (int)hb.walls_list.size();
+    c->max_coll = std::max(c->max_coll, p.N_colloids);
+  }
+  Dev& d = c->d;
+  d.Ntot = Ntot;
+  d.Npad = (Ntot + 31) / 32 * 32;
+  d.nboxes = nboxes;
+  d.Ctot = Ctot;
+  d.ncoll = ncoll;
+  d.nwallseg = nwall;
+  d.Nlist_coll = nlist;
+  d.cap = o.nbr_capacity > 0 ? o.nbr_capacity : derived_capacity(c->boxes, c->dim);
+  c->key_bits = bits_for(std::max(Ctot, 2));
+  const size_t Np = d.Npad;
+  bool ok = true;
+  BoxParams* dbox = nullptr;
+  ok = ok && dalloc(c, &dbox, nboxes);
+  d.box = dbox;
+  ok = ok && dalloc(c, &d.pos, Np) && dalloc(c, &d.vel, Np) && dalloc(c, &d.conf, 6 * Np);
+  ok = ok && dalloc(c, &d.tinfo, Np) && dalloc(c, &d.gid, Np) && dalloc(c, &d.inv, Np);
+  ok = ok && dalloc(c, &d.pos_b, Np) && dalloc(c, &d.vel_b, Np) && dalloc(c, &d.conf_b, 6 * Np);
+  ok = ok && dalloc(c, &d.tinfo_b, Np) && dalloc(c, &d.gid_b, Np);
+  if (c->prec == SPH_PREC_MIXED) ok = ok && dalloc(c, &d.pos_f, Np);
+  ok = ok && dalloc(c, &d.dens, Np) && dalloc(c, &d.press, Np);
+  ok = ok && dalloc(c, &d.f, 3 * Np) && dalloc(c, &d.dcdt, 6 * Np);
+  ok = ok && dalloc(c, &d.f_b, 3 * Np) && dalloc(c, &d.dcdt_b, 6 * Np);
+  ok = ok && dalloc(c, &d.gradv, 9 * Np);
+  if (c->prec == SPH_PREC_MIXED) {
+    RecF* r = nullptr;
+    ok = ok && dalloc(c, &r, Np);
+    d.rec = r;
+  } else {
+    RecD* r = nullptr;
+    ok = ok && dalloc(c, &r, Np);
+    d.rec = r;
+  }
+  ok = ok && dalloc(c, &d.nbr, (size_t)d.cap * Np) && dalloc(c, &d.nbr_cnt, Np);
+  ok = ok && dalloc(c, &d.key_by_gid, Np) && dalloc(c, &d.keys, Np) && dalloc(c, &d.vals, Np);
+  ok = ok && dalloc(c, &d.keys_alt, Np) && dalloc(c, &d.vals_alt, Np);
+  ok = ok && dalloc(c, &d.cell_begin, Ctot + 1) && dalloc(c, &d.cell_start, Ctot);
+  ok = ok && dalloc(c, &d.cell_end, Ctot) && dalloc(c, &d.cell_box, Ctot);
+  ok = ok && dalloc(c, &d.walls_list, nwl) && dalloc(c, &d.wall_seg, nwall + 1);
+  ok = ok && dalloc(c, &d.wall_f, 3 * std::max(nwall, 1));
+  ok = ok && dalloc(c, &d.colloids_list, nlist) && dalloc(c, &d.coll_seg, ncoll + 1);
+  ok = ok && dalloc(c, &d.coll_box, ncoll) && dalloc(c, &d.xc, 3 * (size_t)std::max(nlist, 1));
+  ok = ok && dalloc(c, &d.cs, (size_t)kCollFields * std::max(ncoll, 1));
+  ok = ok && dalloc(c, &d.ccell, ncoll) && dalloc(c, &d.cindex, ncoll);
+  ok = ok && dalloc(c, &d.ccell_start, ncc) && dalloc(c, &d.ccell_end, ncc);
+  ok = ok && dalloc(c, &d.mag, 3 * nboxes) && dalloc(c, &d.ke, nboxes);
+  ok = ok && dalloc(c, &d.step, 1) && dalloc(c, &d.status, 1) && dalloc(c, &d.err_info, 2);
+  ok = ok && dalloc(c, &c->scratch, Np) && dalloc(c, &c->iscratch, Np);
+  c->sort.hist_len = (int)sort_hist_len(Ntot, c->key_bits);
+  ok = ok && dalloc(c, &c->sort.hist, (size_t)c->sort.hist_len);
+  // kinetic-energy chunks
+  std::vector<int> kchunk{0}, kbox{0};
+  for (const HostBox& hb : c->boxes) {
+    for (int s = hb.p.slot0; s < hb.p.slot0 + hb.p.N; s += 4096)
+      kchunk.push_back(std::min(s + 4096, hb.p.slot0 + hb.p.N));
+    kbox.push_back((int)kchunk.size() - 1);
+  }
+  d.nkechunks = (int)kchunk.size() - 1;
+  ok = ok && dalloc(c, &d.ke_chunk, kchunk.size()) && dalloc(c, &d.ke_box_chunk, kbox.size());
+  ok = ok && dalloc(c, &c->ke_partial, std::max(d.nkechunks, 1));
+  if (!ok) {
+    fprintf(stderr, "sph_create: device allocation failed\n");
+    free_ctx(c);
+    return SPH_ERR_NOMEM;
+  }
+  // ---- host images in id order (slot = id at start) ----
+  std::vector<double4> pos(Np), vel(Np);
+  std::vector<double> conf(6 * Np, 0.0);
+  std::vector<int> tinfo(Np, 0), gid(Np, 0), cell_box(Ctot), wl, wseg{0}, cl, cseg{0}, cbox;
+  std::vector<double> xc(3 * (size_t)std::max(nlist, 1), 0.0), cs((size_t)kCollFields * std::max(ncoll, 1), 0.0);
+  std::vector<BoxParams> params;
+  for (int b = 0; b < nboxes; ++b) {
+    const HostBox& hb = c->boxes[b];
+    const BoxParams& p = hb.p;
+    params.push_back(p);
+    for (int i = 0; i < p.N; ++i) {
+      const int s = p.slot0 + i;
+      pos[s] = make_double4(hb.x[i], hb.y[i], hb.z[i], hb.mass[i]);
+      vel[s] = make_double4(hb.vx[i], hb.vy[i], hb.vz[i], 0.0);
+      conf[0 * Np + s] = hb.cxx[i];
+      conf[1 * Np + s] = hb.cxy[i];
+      conf[2 * Np + s] = hb.cyy[i];
+      conf[3 * Np + s] = hb.cxz[i];
+      conf[4 * Np + s] = hb.cyz[i];
+      conf[5 * Np + s] = hb.czz[i];
+      tinfo[s] = (hb.type[i] & kTypeMask) | (b << kTypeBits);
+      gid[s] = s;
+    }
+    for (int q = 0; q < p.Ntotal_cells; ++q) cell_box[p.cell0 + q] = b;
+    if (p.wall) {
+      const int w1 = hb.walls_start[1];
+      for (int k = 0; k < (int)hb.walls_list.size(); ++k) {
+        if (k == w1) wseg.push_back((int)wl.size());
+        wl.push_back(p.slot0 + hb.walls_list[k]);
+      }
+      if ((int)hb.walls_list.size() == w1) wseg.push_back((int)wl.size());
+      wseg.push_back((int)wl.size());
+    }
+    for (int k = 0; k < p.N_colloids; ++k) {
+      const int gc = p.coll0 + k;
+      const int k0 = hb.colloids_start[k];
+      const int k1 = k + 1 < p.N_colloids ? hb.colloids_start[k + 1] : (int)hb.colloids_list.size();
+      for (int q = k0; q < k1; ++q) {
+        const int e = (int)cl.size();
+        cl.push_back(p.slot0 + hb.colloids_list[q]);
+        xc[e] = hb.x_center[q];
+        xc[(size_t)std::max(nlist, 1) + e] = hb.y_center[q];
+        xc[2 * (size_t)std::max(nlist, 1) + e] = hb.z_center[q];
+      }
+      cseg.push_back((int)cl.size());
+      cbox.push_back(b);
+      cs[CS_X * ncoll + gc] = hb.coll_x[k];
+      cs[CS_Y * ncoll + gc] = hb.coll_y[k];
+      cs[CS_Z * ncoll + gc] = hb.coll_z[k];
+      cs[CS_Q0 * ncoll + gc] = 1.0;
+    }
+  }
+  if (Ntot > 0 && (int)tinfo.size() > 0 && nboxes >= (1 << (31 - kTypeBits))) ok = false;
+  auto up = [&](void* dst, const void* src, size_t bytes) {
+    if (bytes && cudaMemcpyAsync(dst, src, bytes, cudaMemcpyHostToDevice, c->stream) != cudaSuccess)
+      ok = false;
+  };
+  up((void*)d.box, params.data(), params.size() * sizeof(BoxParams));
+  up(d.pos, pos.data(), Np * sizeof(double4));
+  up(d.vel, vel.data(), Np * sizeof(double4));
+  up(d.conf, conf.data(), conf.size() * sizeof(double));
+  up(d.tinfo, tinfo.data(), Np * sizeof(int));
+  up(d.gid, gid.data(), Np * sizeof(int));
+  up(d.inv, gid.data(), Np * sizeof(int));
+  up(d.cell_box, cell_box.data(), cell_box.size() * sizeof(int));
+  up(d.walls_list, wl.data(), wl.size() * sizeof(int));
+  up(d.wall_seg, wseg.data(), wseg.size() * sizeof(int));
+  up(d.colloids_list, cl.data(), cl.size() * sizeof(int));
+  up(d.coll_seg, cseg.data(), cseg.size() * sizeof(int));
+  up(d.coll_box, cbox.data(), cbox.size() * sizeof(int));
+  up(d.xc, xc.data(), xc.size() * sizeof(double));
+  up(d.cs, cs.data(), cs.size() * sizeof(double));
+  up(d.ke_chunk, kchunk.data(), kchunk.size() * sizeof(int));
+  up(d.ke_box_chunk, kbox.data(), kbox.size() * sizeof(int));
+  if (!ok || cudaStreamSynchronize(c->stream) != cudaSuccess) {
+    fprintf(stderr, "sph_create: upload failed: %s\n", cudaGetErrorString(cudaGetLastError()));
+    free_ctx(c);
+    return SPH_ERR_CUDA;
+  }
+  *out = c;
+  return SPH_OK;
+}
+
+sph_status sph_create(const sph_input* in, const char* particles_path, const sph_options* opt,
+                      sph_ctx** out) {
+  const char* paths[1] = {particles_path};
+  return sph_create_ensemble(1, in, paths, opt, out);
+}
+
+void sph_destroy(sph_ctx* ctx) {
+  if (!ctx) return;
+  cudaSetDevice(ctx->device);
+  cudaStreamSynchronize(ctx->stream);
+  free_ctx(ctx);
+}
+
+sph_status sph_get_info(const sph_ctx* c, int box, sph_info* o) {
+  if (!c || !o || box < 0 || box >= c->nboxes) return SPH_ERR_STATE;
+  const HostBox& hb = c->boxes[box];
+  const BoxParams& p = hb.p;
+  std::memset(o, 0, sizeof(*o));
+  o->N = p.N;
+  o->dim = p.dim;
+  o->wall = p.wall;
+  for (int q = 0; q < 3; ++q) {
+    o->Ncells[q] = p.Ncells[q];
+    o->Ncells_colloids[q] = p.Ncells_colloids[q];
+    o->cell_size[q] = p.cell_size[q];
+    o->L[q] = p.L[q];
+  }
+  o->Ntotal_cells = p.Ntotal_cells;
+  o->Nwalls = p.wall ? 2 : 0;
+  o->Nlist_walls = (int)hb.walls_list.size();
+  o->N_colloids = p.N_colloids;
+  o->Nlist_colloids = (int)hb.colloids_list.size();
+  o->Ntotal_cells_colloids = p.Ntotal_cells_colloids;
+  o->step = (int)c->host_step;
+  o->nboxes = c->nboxes;
+  o->precision = c->prec;
+  o->rcut = p.rcut;
+  o->rcutsq = p.rcutsq;
+  o->cw = p.cw;
+  o->c_gradw = p.c_gradw;
+  o->csq = p.csq;
+  o->rho0 = p.rho0;
+  o->a = p.a;
+  o->b = p.b;
+  o->nkT = p.nkT;
+  o->tau = p.tau;
+  o->dt = p.dt;
+  o->wall_width = p.wall_width;
+  o->y_bottom = p.y_bottom;
+  o->y_top = p.y_top;
+  o->V_bottom = p.V_bottom;
+  o->V_top = p.V_top;
+  o->coll_R = p.coll_R;
+  o->coll_mass = p.coll_mass;
+  o->coll_I = p.coll_I;
+  o->t0 = p.t0;
+  o->omega_magnet = p.omega_magnet;
+  return SPH_OK;
+}
+
+// ---- class_system methods ----
+#define CTX_GUARD(c)                  \
+  if (!(c)) return SPH_ERR_STATE;     \
+  cudaSetDevice((c)->device);
+
+sph_status sph_neighbours_search(sph_ctx* c) {
+  CTX_GUARD(c);
+  return search_checked(c);
+}
+
+sph_status sph_calculate_density(sph_ctx* c) {
+  CTX_GUARD(c);
+  sph_status s = ensure_lists(c);
+  if (s != SPH_OK) return s;
+  if (launch_density_dim(launcher(c), c->dim)) return cuda_fail(c, "calculate_density");
+  return SPH_OK;
+}
+
+sph_status sph_calculate_pressure(sph_ctx* c) {
+  CTX_GUARD(c);
+  if (launch_pressure(launcher(c))) return cuda_fail(c, "calculate_pressure");
+  return SPH_OK;
+}
+
+sph_status sph_calculate_vel_gradient(sph_ctx* c) {
+  CTX_GUARD(c);
+  sph_status s = ensure_lists(c);
+  if (s != SPH_OK) return s;
+  // the pair pass reads the neighbour records, refreshed from the current state
+  if (launch_pressure(launcher(c))) return cuda_fail(c, "records");
+  if (launch_pairs_dim(launcher(c), c->dim, kPairGradvAll, 0)) return cuda_fail(c, "vel_gradient");
+  c->gradv_valid = true;
+  return SPH_OK;
+}
+
+sph_status sph_calculate_forces(sph_ctx* c, const double* m) {
+  CTX_GUARD(c);
+  sph_status s = ensure_lists(c);
+  if (s != SPH_OK) return s;
+  s = m ? upload_moment(c, m) : host_moment(c, c->host_step + (c->in_step ? 1 : 0));
+  if (s != SPH_OK) return s;
+  Launch L = launcher(c);
+  bool ext = false;
+  for (const HostBox& hb : c->boxes) ext = ext || hb.p.ext_force_type != 0;
+  // the reference stores the velocity gradient of every particle in this call
+  if (launch_density_dim(L, c->dim) || launch_pairs_dim(L, c->dim, kPairGradvAll, 0) ||
+      launch_pairs_dim(L, c->dim, kPairFused, ext ? 1 : 0) || launch_wall_forces(L))
+    return cuda_fail(c, "calculate_forces");
+  bool pairs = false;
+  for (const HostBox& hb : c->boxes) pairs = pairs || hb.p.N_colloids >= 2;
+  if (launch_colloid_forces(L, pairs ? 1 : 0)) return cuda_fail(c, "calculate_forces");
+  c->forces_live = true;
+  c->gradv_valid = true;
+  return SPH_OK;
+}
+
+sph_status sph_calculate_external_forces(sph_ctx* c) {
+  CTX_GUARD(c);
+  if (launch_ext_force(launcher(c))) return cuda_fail(c, "external forces");
+  return SPH_OK;
+}
+
+sph_status sph_calculate_force_walls(sph_ctx* c) {
+  CTX_GUARD(c);
+  if (launch_wall_forces(launcher(c))) return cuda_fail(c, "force_walls");
+  return SPH_OK;
+}
+
+sph_status sph_calculate_force_colloids(sph_ctx* c, const double* m) {
+  CTX_GUARD(c);
+  sph_status s = m ? upload_moment(c, m) : host_moment(c, c->host_step + (c->in_step ? 1 : 0));
+  if (s != SPH_OK) return s;
+  if (c->pos_dirty) {
+    s = search_checked(c);
+    if (s != SPH_OK) return s;
+  }
+  bool pairs = false;
+  for (const HostBox& hb : c->boxes) pairs = pairs || hb.p.N_colloids >= 2;
+  if (launch_colloid_forces(launcher(c), pairs ? 1 : 0)) return cuda_fail(c, "force_colloids");
+  return SPH_OK;
+}
+
+sph_status sph_vv_step1(sph_ctx* c) {
+  CTX_GUARD(c);
+  if (ph_vv1(c)) return cuda_fail(c, "V_Verlet_step1");
+  c->in_step = true;
+  return SPH_OK;
+}
+
+sph_status sph_vv_step2(sph_ctx* c) {
+  CTX_GUARD(c);
+  if (ph_vv2(c)) return cuda_fail(c, "V_Verlet_step2");
+  c->host_step++;
+  c->in_step = false;
+  return SPH_OK;
+}
+
+sph_status sph_initial_forces(sph_ctx* c) {
+  CTX_GUARD(c);
+  return do_initial(c);
+}
+
+sph_status sph_step(sph_ctx* c, int nsteps) {
+  CTX_GUARD(c);
+  if (nsteps < 0) return SPH_ERR_STATE;
+  if (!c->initial_done) {
+    sph_status s = do_initial(c);
+    if (s != SPH_OK) return s;
+  }
+  if (c->in_step) return fail(c, SPH_ERR_STATE, "sph_step inside a half-finished step");
+  if (nsteps == 0) return SPH_OK;
+  if (c->use_graph && !c->graph[0]) {
+    sph_status s = capture_graphs(c);
+    if (s != SPH_OK) return s;
+  }
+  cudaEventRecord(c->ev0, c->stream);
+  for (int k = 0; k < nsteps; ++k) {
+    if (c->use_graph) {
+      if (cudaGraphLaunch(c->graph[c->parity], c->stream) != cudaSuccess)
+        return cuda_fail(c, "graph launch");
+      swap_state(c, false);
+      c->launches += c->graph_kernels;
+    } else if (ph_step(c)) {
+      return cuda_fail(c, "step");
+    }
+    c->host_step++;
+  }
+  c->forces_live = true;
+  c->pos_dirty = false;
+  cudaEventRecord(c->ev1, c->stream);
+  c->events_recorded = true;
+  return SPH_OK;
+}
+
+sph_status sph_synchronize(sph_ctx* c) {
+  CTX_GUARD(c);
+  if (cudaStreamSynchronize(c->stream) != cudaSuccess) return cuda_fail(c, "synchronize");
+  if (c->events_recorded) {
+    float ms = 0.f;
+    if (cudaEventElapsedTime(&ms, c->ev0, c->ev1) == cudaSuccess) c->last_ms = ms;
+    c->events_recorded = false;
+  }
+  sph_status s = check_device(c);
+  if (s == SPH_OK) {
+    int info[2];
+    cudaMemcpy(info, c->d.err_info, sizeof(info), cudaMemcpyDeviceToHost);
+    // keep headroom: grow the lists (and recapture) once 90% of the capacity is in use
+    if (info[1] > (9 * c->d.cap) / 10) s = grow_capacity(c, info[1]);
+  }
+  return s;
+}
+
+sph_status sph_last_step_ms(sph_ctx* c, double* ms) {
+  if (!c || !ms) return SPH_ERR_STATE;
+  *ms = c->last_ms;
+  return SPH_OK;
+}
+
+sph_status sph_kernel_launches(const sph_ctx* c, long long* count) {
+  if (!c || !count) return SPH_ERR_STATE;
+  *count = c->launches;
+  return SPH_OK;
+}
+
+// ---- state access ----
+sph_status sph_read_field_device(sph_ctx* c, int field, double* dev_out) {
+  CTX_GUARD(c);
+  if (field < 0 || field >= SPH_NUM_PARTICLE_FIELDS || !dev_out) return SPH_ERR_STATE;
+  if (field >= SPH_GXX && field <= SPH_GZZ && !c->gradv_valid) {
+    if (sph_calculate_vel_gradient(c) != SPH_OK) return SPH_ERR_CUDA;
+  }
+  if (launch_gather_field(launcher(c), field, dev_out)) return cuda_fail(c, "read_field");
+  return SPH_OK;
+}
+
+sph_status sph_read_field(sph_ctx* c, int field, double* host_out) {
+  CTX_GUARD(c);
+  if (!host_out) return SPH_ERR_STATE;
+  sph_status s = sph_read_field_device(c, field, c->scratch);
+  if (s != SPH_OK) return s;
+  if (cudaMemcpyAsync(host_out, c->scratch, (size_t)c->d.Ntot * sizeof(double),
+                      cudaMemcpyDeviceToHost, c->stream) != cudaSuccess ||
+      cudaStreamSynchronize(c->stream) != cudaSuccess)
+    return cuda_fail(c, "read_field copy");
+  return SPH_OK;
+}
+
+sph_status sph_write_field(sph_ctx* c, int field, const double* host_in) {
+  CTX_GUARD(c);
+  if (field < 0 || field >= SPH_NUM_PARTICLE_FIELDS || !host_in) return SPH_ERR_STATE;
+  if (cudaMemcpyAsync(c->scratch, host_in, (size_t)c->d.Ntot * sizeof(double),
+                      cudaMemcpyHostToDevice, c->stream) != cudaSuccess)
+    return cuda_fail(c, "write_field copy");
+  if (launch_scatter_field(launcher(c), field, c->scratch)) return cuda_fail(c, "write_field");
+  if (field <= SPH_Z) c->pos_dirty = true;
+  drop_graphs(c);
+  cudaStreamSynchronize(c->stream);
+  return SPH_OK;
+}
+
+sph_status sph_read_type(sph_ctx* c, int* host_out) {
+  CTX_GUARD(c);
+  if (!host_out) return SPH_ERR_STATE;
+  if (launch_gather_int(launcher(c), c->d.tinfo, c->iscratch)) return cuda_fail(c, "read_type");
+  std::vector<int> t(c->d.Ntot);
+  if (cudaMemcpyAsync(t.data(), c->iscratch, t.size() * sizeof(int), cudaMemcpyDeviceToHost,
+                      c->stream) != cudaSuccess ||
+      cudaStreamSynchronize(c->stream) != cudaSuccess)
+    return cuda_fail(c, "read_type copy");
+  for (size_t i = 0; i < t.size(); ++i) host_out[i] = t[i] & kTypeMask;
+  return SPH_OK;
+}
+
+sph_status sph_read_colloid_field(sph_ctx* c, int field, double* host_out) {
+  CTX_GUARD(c);
+  if (field < 0 || field >= SPH_NUM_COLLOID_FIELDS || !host_out) return SPH_ERR_STATE;
+  if (c->d.ncoll == 0) return SPH_OK;
+  if (cudaMemcpyAsync(host_out, c->d.cs + (size_t)field * c->d.ncoll,
+                      (size_t)c->d.ncoll * sizeof(double), cudaMemcpyDeviceToHost,
+                      c->stream) != cudaSuccess ||
+      cudaStreamSynchronize(c->stream) != cudaSuccess)
+    return cuda_fail(c, "read_colloid_field");
+  return SPH_OK;
+}
+
+sph_status sph_read_wall_forces(sph_ctx* c, double* host_out) {
+  CTX_GUARD(c);
+  if (!host_out) return SPH_ERR_STATE;
+  std::vector<double> wf(3 * (size_t)std::max(c->d.nwallseg, 1));
+  if (c->d.nwallseg > 0 &&
+      (cudaMemcpyAsync(wf.data(), c->d.wall_f, 3 * (size_t)c->d.nwallseg * sizeof(double),
+                       cudaMemcpyDeviceToHost, c->stream) != cudaSuccess ||
+       cudaStreamSynchronize(c->stream) != cudaSuccess))
+    return cuda_fail(c, "read_wall_forces");
+  for (int b = 0; b < c->nboxes; ++b) {
+    const BoxParams& p = c->boxes[b].p;
+    for (int q = 0; q < 6; ++q)
+      host_out[6 * b + q] = p.wall ? wf[3 * (size_t)p.wall_seg0 + q] : 0.0;
+  }
+  return SPH_OK;
+}
+
+sph_status sph_export_cells(sph_ctx* c, int* particle_cell, int* particle_index,
+                            int* cell_start, int* cell_end) {
+  CTX_GUARD(c);
+  const BoxParams& p = c->boxes[0].p;
+  cudaStream_t st = c->stream;
+  bool ok = true;
+  auto dn = [&](void* dst, const void* src, size_t bytes) {
+    if (dst && cudaMemcpyAsync(dst, src, bytes, cudaMemcpyDeviceToHost, st) != cudaSuccess) ok = false;
+  };
+  dn(particle_cell, c->d.keys + p.slot0, (size_t)p.N * sizeof(int));
+  dn(particle_index, c->d.vals + p.slot0, (size_t)p.N * sizeof(int));
+  dn(cell_start, c->d.cell_start + p.cell0, (size_t)p.Ntotal_cells * sizeof(int));
+  dn(cell_end, c->d.cell_end + p.cell0, (size_t)p.Ntotal_cells * sizeof(int));
+  if (!ok || cudaStreamSynchronize(st) != cudaSuccess) return cuda_fail(c, "export_cells");
+  return SPH_OK;
+}
+
+sph_status sph_export_colloid_cells(sph_ctx* c, int* coll_cell, int* coll_index,
+                                    int* coll_cell_start, int* coll_cell_end) {
+  CTX_GUARD(c);
+  const BoxParams& p = c->boxes[0].p;
+  if (p.N_colloids == 0) return SPH_OK;
+  cudaStream_t st = c->stream;
+  bool ok = true;
+  auto dn = [&](void* dst, const void* src, size_t bytes) {
+    if (dst && cudaMemcpyAsync(dst, src, bytes, cudaMemcpyDeviceToHost, st) != cudaSuccess) ok = false;
+  };
+  dn(coll_cell, c->d.ccell + p.coll0, (size_t)p.N_colloids * sizeof(int));
+  dn(coll_index, c->d.cindex + p.coll0, (size_t)p.N_colloids * sizeof(int));
+  dn(coll_cell_start, c->d.ccell_start + p.ccell0, (size_t)p.Ntotal_cells_colloids * sizeof(int));
+  dn(coll_cell_end, c->d.ccell_end + p.ccell0, (size_t)p.Ntotal_cells_colloids * sizeof(int));
+  if (!ok || cudaStreamSynchronize(st) != cudaSuccess) return cuda_fail(c, "export_colloid_cells");
+  return SPH_OK;
+}
+
+sph_status sph_kinetic_energy(sph_ctx* c, double* host_out) {
+  CTX_GUARD(c);
+  if (!host_out) return SPH_ERR_STATE;
+  if (launch_kinetic_energy(launcher(c), c->ke_partial)) return cuda_fail(c, "kinetic_energy");
+  if (cudaMemcpyAsync(host_out, c->d.ke, (size_t)c->nboxes * sizeof(double),
+                      cudaMemcpyDeviceToHost, c->stream) != cudaSuccess ||
+      cudaStreamSynchronize(c->stream) != cudaSuccess)
+    return cuda_fail(c, "kinetic_energy copy");
+  return SPH_OK;
+}
+
+}  // extern "C"

@@ -1,0 +1,218 @@
+// sph_internal.h -- engine-internal types shared by the host setup, the kernels and the
+// C-ABI layer.  Nothing here is part of the public interface (include/sph_capi.h).
+#pragma once
+
+#include <cstdint>
+#include <string>
+#include <vector>
+
+#include <vector_types.h>
+
+#include "sph_capi.h"
+
+namespace sph {
+
+// Particle type word: type in the low 12 bits (0 fluid, 1 bottom wall, 2 top wall,
+// 3 + k colloid k of its box), box index above.  One int per particle carries both.
+constexpr int kTypeBits = 12;
+constexpr int kTypeMask = (1 << kTypeBits) - 1;
+
+// Device error flags (bit set in Ctx::d_status by any kernel that detects the condition).
+enum StatusBits : unsigned {
+  kStatCellRange = 1u, // hash outside the grid (reference traps: kernel_cell_ranges.cu:20-23)
+  kStatNaN = 2u,       // non-finite position
+  kStatCapacity = 4u,  // neighbour list full
+};
+
+// Per-box constants.  Everything the reference keeps in __constant__ memory
+// (src/kernel_declare_constants.cu:11-62) plus the box's offsets in the global arrays.
+struct BoxParams {
+  int dim, wall, ext_force_type, coll_move;
+  int N;           // particles in this box
+  int slot0;       // first slot (and first global id) of the box
+  int cell0;       // first global cell index of the box
+  int Ncells[3], Ntotal_cells;
+  int N_colloids, coll0;  // colloids of the box and their first global index
+  int wall_seg0;          // first of the box's two wall segments
+  int pad0;
+  double L[3], halfL[3], cell_size[3], wall_width;
+  double rcut, rcutsq, rcut_inv, cw, c_gradw, csq, rho0, a, b, nkT, tau, dt;
+  double ext_force[3], ky;
+  double y_bottom, y_top, V_bottom, V_top, beta_max;
+  double coll_R, coll_rho, coll_mass, coll_I;
+  double F0_rep, tau_rep, rcuton_coll_rep_sq, rcutoff_coll_rep_sq, r0_magnet_sq, F0_magnet;
+  double omega_magnet, t0;
+  double list_cut2;  // squared list cutoff used by the float candidate test
+  // colloid coarse grid (only exported; pair forces loop over all colloids of the box)
+  int Ncells_colloids[3], Ntotal_cells_colloids;
+  double cell_colloids_size[3];
+  int ccell0;  // first global coarse-cell index of the box
+  int pad1;
+};
+
+// Host-side description of one box after setup (original particle order), produced by
+// the host setup (sph_setup.cpp) and uploaded by the context.
+struct HostBox {
+  BoxParams p;
+  sph_input in;
+  std::vector<double> coll_xyz;  // storage behind in.coll_xyz
+  // particles (original order)
+  std::vector<double> x, y, z, vx, vy, vz, mass, cxx, cxy, cyy, cxz, cyz, czz;
+  std::vector<int> type;
+  // walls_list / walls_start (system_initialize.cpp:278-300), local ids
+  std::vector<int> walls_list;
+  int walls_start[2] = {0, 0};
+  int Nlist_walls = 0;
+  // colloids (system_initialize.cpp:176-201, 304-355)
+  std::vector<int> colloids_list, colloids_start;
+  std::vector<double> x_center, y_center, z_center;
+  std::vector<double> coll_x, coll_y, coll_z;
+};
+
+// Parses a reference `input` file.  Returns SPH_OK or SPH_ERR_BAD_INPUT / SPH_ERR_IO.
+sph_status parse_input_file(const char* path, sph_input* in, std::vector<double>* coll,
+                            std::string* msg);
+// Builds a box from its inputs (constructor + initialize of the reference).
+sph_status build_box(const sph_input& in, const char* particles_path, HostBox* box,
+                     std::string* msg);
+
+// Neighbour-record layouts (one per particle, slot order), written by the density
+// epilogue and gathered by the pair kernel.  P holds Pi/d^2 = (p I - nkT c)/d^2 for
+// fluid particles and -nkT c for walls and colloid particles (whose Pi is rebuilt with
+// the fluid partner's pressure and density, kernel_forces.cu:217-233).
+struct alignas(16) RecD {
+  double x, y, z, vx, vy, vz;
+  double P[6];
+  double invd;
+  int tinfo;
+  int pad;
+  double pad2[2];
+};
+static_assert(sizeof(RecD) == 128, "RecD layout");
+
+struct alignas(16) RecF {
+  float x, y, z, vx, vy, vz;
+  float P[6];
+  float invd;
+  int tinfo;
+  float pad[2];
+};
+static_assert(sizeof(RecF) == 64, "RecF layout");
+
+// Device pointers, passed to kernels by value.
+struct Dev {
+  int Ntot, Npad, nboxes, Ctot, ncoll, nwallseg, cap;
+  const BoxParams* box;
+  double4* pos;  // x, y, z, mass
+  double4* vel;  // vx, vy, vz, 0
+  double* conf;  // 6 x Npad: cxx, cxy, cyy, cxz, cyz, czz
+  int* tinfo;    // type | box << kTypeBits
+  int* gid;      // slot -> global particle id
+  int* inv;      // global id -> slot
+  double4* pos_b;
+  double4* vel_b;
+  double* conf_b;
+  int* tinfo_b;
+  int* gid_b;
+  float4* pos_f;  // float copy of pos (mixed precision only), slot order
+  double* dens;
+  double* press;
+  double* f;     // 3 x Npad
+  double* dcdt;  // 6 x Npad
+  double* f_b;   // reorder targets of f / dcdt when a search falls between
+  double* dcdt_b;  // a force evaluation and the half-kick that consumes it
+  double* gradv; // 9 x Npad: xx xy xz yx yy yz zx zy zz
+  void* rec;     // RecD or RecF per slot
+  int* nbr;      // cap x Npad, column major
+  int* nbr_cnt;  // per slot
+  int* key_by_gid;
+  int* keys;     // sorted keys
+  int* vals;     // sorted values (global ids)
+  int* keys_alt;
+  int* vals_alt;
+  int* cell_begin;     // Ctot + 1: first slot of each global cell (current)
+  int* cell_start;     // Ctot, reference semantics, box-local slot index
+  int* cell_end;       // Ctot
+  int* cell_box;       // Ctot: owning box of each global cell
+  // walls
+  int* walls_list;     // global ids
+  int* wall_seg;       // nwallseg + 1 segment boundaries into walls_list
+  double* wall_f;      // nwallseg x 3
+  // colloids
+  int* colloids_list;  // global ids
+  int* coll_seg;       // ncoll + 1 segment boundaries into colloids_list
+  int* coll_box;       // ncoll
+  double* xc;          // body-frame offsets per colloids_list entry (3 x Nlist)
+  int Nlist_coll;
+  double* cs;          // colloid state, kCollFields x ncoll
+  int* ccell;          // colloid coarse-grid arrays (reference semantics), ncoll
+  int* cindex;
+  int* ccell_start;    // sum of coarse cells over boxes
+  int* ccell_end;
+  double* mag;         // 3 x nboxes magnetic moments
+  double* ke;          // nboxes
+  int* ke_chunk;       // nkechunks + 1 slot boundaries, chunks never straddle boxes
+  int* ke_box_chunk;   // nboxes + 1 chunk boundaries per box
+  int nkechunks;
+  long long* step;     // device step counter (graph replays)
+  unsigned* status;
+  int* err_info;       // [0] first bad slot, [1] largest neighbour count seen
+};
+
+// Colloid state layout in Dev::cs (each row ncoll long).
+enum CollField {
+  CS_X = 0, CS_Y, CS_Z, CS_VX, CS_VY, CS_VZ, CS_OX, CS_OY, CS_OZ, CS_THETA, CS_Q0, CS_QX,
+  CS_QY, CS_QZ, CS_FX, CS_FY, CS_FZ, CS_TX, CS_TY, CS_TZ, kCollFields
+};
+
+// Kernel launchers (sph_kernels.cu); all asynchronous on `stream`.
+struct Launch {
+  Dev d;
+  int prec;  // sph_precision
+  void* stream;
+  long long* launches;
+};
+
+enum PairMode { kPairFused = 0, kPairGradvAll = 1, kPairForcesOnly = 2 };
+
+// CUDA error code of the most recent failed launch on this thread (0 = none); the
+// launchers clear the runtime's last-error state, so the code is kept here for reporting.
+inline int& last_launch_error() {
+  static thread_local int e = 0;
+  return e;
+}
+
+int launch_vv1_particles(const Launch& L);
+int launch_vv1_colloids(const Launch& L);
+int launch_vv2(const Launch& L);
+int launch_hash(const Launch& L);
+int launch_reorder(const Launch& L, bool permute_forces);
+int launch_build_lists_dim(const Launch& L, int dim);
+int launch_colloid_cells_n(const Launch& L, int nboxes, int max_coll);
+int launch_density_dim(const Launch& L, int dim);
+int launch_pressure(const Launch& L);
+int launch_pairs_dim(const Launch& L, int dim, int mode, int with_ext);
+int launch_ext_force(const Launch& L);
+int launch_dcdt_from_gradv(const Launch& L);
+int launch_wall_forces(const Launch& L);
+int launch_colloid_forces(const Launch& L, int with_pairs);
+int launch_advance_time(const Launch& L, int mode);
+int launch_count_step(const Launch& L);
+int launch_kinetic_energy(const Launch& L, double* partial);
+int launch_gather_field(const Launch& L, int field, double* out);
+int launch_scatter_field(const Launch& L, int field, const double* in);
+int launch_gather_int(const Launch& L, const int* src, int* out);
+
+// Stable LSD radix sort of the hash keys (sph_sort.cu): keys d.key_by_gid indexed by
+// global id, values = global ids; result in d.keys / d.vals.
+struct SortScratch {
+  int* hist;       // radix histogram / offsets
+  int hist_len;
+  int ntiles;
+};
+size_t sort_hist_len(int n, int key_bits);
+int launch_sort(const Launch& L, int key_bits, const SortScratch& scr);
+
+size_t sort_hist_len(int n, int key_bits);
+
+}  // namespace sph

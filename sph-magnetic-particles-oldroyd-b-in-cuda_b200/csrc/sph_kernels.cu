@@ -1,0 +1,1562 @@
+// sph_kernels.cu -- device kernels of the SPH step for sm_100a.
+//
+// Layout: particles live in "slot" order, the stable (cell, id) order of the last
+// neighbour search, so that every cell's particles are contiguous in HBM.  State is SoA /
+// packed AoS (pos = double4 x,y,z,mass; vel = double4) and is permuted into the new order
+// once per search (k_reorder).  The pair phases read per-particle neighbour lists built by
+// a warp-per-cell kernel (k_build_lists) that walks the 3^d neighbour cells in the
+// reference's order (kernel_densities.cu:52-163), so each particle's sums run over the
+// same neighbours in the same order as the reference's gather loops.  All sums are
+// gathers (no atomics), so results are bit-reproducible run to run.
+#include <cuda_runtime.h>
+#include <math.h>
+#include <stdint.h>
+
+#include "sph_internal.h"
+
+namespace sph {
+
+#define SPH_FULL 0xffffffffu
+
+__device__ __forceinline__ int type_of(int t) { return t & kTypeMask; }
+__device__ __forceinline__ int box_of(int t) { return t >> kTypeBits; }
+
+template <typename T> struct V4;
+template <> struct V4<double> { using type = double4; };
+template <> struct V4<float> { using type = float4; };
+
+template <typename T> struct RecOf;
+template <> struct RecOf<double> { using type = RecD; };
+template <> struct RecOf<float> { using type = RecF; };
+
+// ---------------------------------------------------------------------------------
+// SPH kernel and its radial derivative (kernel_W.cu:13-59, kernel_gradW.cu:13-53).
+// Written branch-free: the clamped terms are exact zeros where the reference skips
+// them, so the value is the same as the branchy form.
+// ---------------------------------------------------------------------------------
+template <typename T>
+__device__ __forceinline__ T sph_w(T r, T rcut_inv, T cw) {
+  T q3 = (r * rcut_inv) * T(3);
+  T t1 = T(3) - q3, t2 = T(2) - q3, t3 = T(1) - q3;
+  T a1 = t1 * t1, a2 = t2 * t2, a3 = t3 * t3;
+  T w = (a1 * a1) * t1;
+  if (q3 < T(2)) w = w - T(6) * ((a2 * a2) * t2);
+  if (q3 < T(1)) w = w + T(15) * ((a3 * a3) * t3);
+  return cw * w;
+}
+
+template <typename T>
+__device__ __forceinline__ T sph_gradw(T r, T rcut_inv, T c_gradw) {
+  T q3 = T(3) * (r * rcut_inv);
+  T t1 = T(3) - q3, t2 = T(2) - q3, t3 = T(1) - q3;
+  T a1 = t1 * t1, a2 = t2 * t2, a3 = t3 * t3;
+  T g = a1 * a1;
+  if (q3 < T(2)) g = g - T(6) * (a2 * a2);
+  if (q3 < T(1)) g = g + T(15) * (a3 * a3);
+  return c_gradw * g;
+}
+
+// Minimum image as the reference writes it: subtract L above L/2, add L below -L/2
+// (kernel_densities.cu:90-110).  y is periodic only without walls; z only in 3D.
+template <typename T, int DIM>
+__device__ __forceinline__ void min_image(T& rx, T& ry, T& rz, const T L[3], const T h[3],
+                                          int wall) {
+  if (rx > h[0]) rx -= L[0];
+  if (rx < -h[0]) rx += L[0];
+  if (!wall) {
+    if (ry > h[1]) ry -= L[1];
+    if (ry < -h[1]) ry += L[1];
+  }
+  if (DIM == 3) {
+    if (rz > h[2]) rz -= L[2];
+    if (rz < -h[2]) rz += L[2];
+  }
+}
+
+// Cell of a position as kernel_cell_list.cu:15-63 computes it (with its clamp rules).
+// Returns the box-local linear cell, or -1 when the reference would assert
+// (kernel_cell_ranges.cu:20-23) or the position is not finite.
+__device__ __forceinline__ int hash_cell(const BoxParams& p, double x, double y, double z) {
+  if (!isfinite(x) || !isfinite(y) || (p.dim == 3 && !isfinite(z))) return -2;
+  int cx = (int)floor(x / p.cell_size[0]);
+  if (cx == p.Ncells[0]) cx = cx - 1;
+  int cy;
+  if (p.wall == 0) {
+    cy = (int)floor(y / p.cell_size[1]);
+    if (cy == p.Ncells[1]) cy = cy - 1;
+  } else {
+    cy = (int)floor((y + p.wall_width) / p.cell_size[1]);
+  }
+  int c;
+  if (p.dim == 3) {
+    int cz = (int)floor(z / p.cell_size[2]);
+    if (cz == p.Ncells[2]) cz = cz - 1;
+    c = cz * p.Ncells[0] * p.Ncells[1] + cy * p.Ncells[0] + cx;
+  } else {
+    c = cy * p.Ncells[0] + cx;
+  }
+  if (c < 0 || c > p.Ntotal_cells - 1) return -1;
+  return c;
+}
+
+// The cell the pair kernels of the reference iterate around: unclamped floor
+// (kernel_densities.cu:52-60).
+__device__ __forceinline__ void own_cell(const BoxParams& p, double x, double y, double z,
+                                         int& cx, int& cy, int& cz) {
+  cx = (int)floor(x / p.cell_size[0]);
+  cy = p.wall == 0 ? (int)floor(y / p.cell_size[1])
+                   : (int)floor((y + p.wall_width) / p.cell_size[1]);
+  cz = p.dim == 3 ? (int)floor(z / p.cell_size[2]) : 0;
+}
+
+__device__ __forceinline__ void raise_status(const Dev& d, unsigned bit, int info) {
+  unsigned old = atomicOr(d.status, bit);
+  if (!(old & bit) && bit != kStatCapacity) atomicExch(&d.err_info[0], info);
+}
+
+// ---------------------------------------------------------------------------------
+// Velocity Verlet, particles (kernel_move_sys_VV_part1.cu:13-114, ..._part2.cu:13-58)
+// ---------------------------------------------------------------------------------
+__global__ void k_vv1_particles(Dev d) {
+  int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= d.Ntot) return;
+  int ti = d.tinfo[i];
+  int t = type_of(ti);
+  if (t > 2) return;  // colloid particles are placed by k_vv1_colloids
+  const BoxParams& p = d.box[box_of(ti)];
+  const double dt = p.dt;
+  double4 x = d.pos[i];
+  double4 v = d.vel[i];
+  const int Np = d.Npad;
+  if (t == 0) {
+    double h = 0.5 * dt;
+    double hm = h / x.w;
+    v.x = v.x + hm * d.f[i];
+    v.y = v.y + hm * d.f[Np + i];
+    d.conf[i] = d.conf[i] + h * d.dcdt[i];
+    d.conf[Np + i] = d.conf[Np + i] + h * d.dcdt[Np + i];
+    d.conf[2 * Np + i] = d.conf[2 * Np + i] + h * d.dcdt[2 * Np + i];
+    if (p.dim == 3) {
+      v.z = v.z + hm * d.f[2 * Np + i];
+      d.conf[3 * Np + i] = d.conf[3 * Np + i] + h * d.dcdt[3 * Np + i];
+      d.conf[4 * Np + i] = d.conf[4 * Np + i] + h * d.dcdt[4 * Np + i];
+      d.conf[5 * Np + i] = d.conf[5 * Np + i] + h * d.dcdt[5 * Np + i];
+    }
+  } else {
+    v.x = (t == 1) ? p.V_bottom : p.V_top;
+    v.y = 0.0;
+    if (p.dim == 3) v.z = 0.0;
+  }
+  double xi = x.x + v.x * dt;
+  double yi = x.y + v.y * dt;
+  double zi = x.z;
+  if (p.dim == 3) zi = x.z + v.z * dt;
+  if (xi < 0) xi = xi + p.L[0];
+  if (p.wall == 0 && yi < 0) yi = yi + p.L[1];
+  if (p.dim == 3 && zi < 0) zi = zi + p.L[2];
+  if (xi > p.L[0]) xi = xi - p.L[0];
+  if (p.wall == 0 && yi > p.L[1]) yi = yi - p.L[1];
+  if (p.dim == 3 && zi > p.L[2]) zi = zi - p.L[2];
+  x.x = xi;
+  x.y = yi;
+  x.z = zi;
+  d.pos[i] = x;
+  d.vel[i] = v;
+}
+
+__global__ void k_vv2_particles(Dev d) {
+  int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= d.Ntot) return;
+  int ti = d.tinfo[i];
+  if (type_of(ti) != 0) return;
+  const BoxParams& p = d.box[box_of(ti)];
+  const int Np = d.Npad;
+  double h = 0.5 * p.dt;
+  double hm = h / d.pos[i].w;
+  double4 v = d.vel[i];
+  v.x = v.x + hm * d.f[i];
+  v.y = v.y + hm * d.f[Np + i];
+  d.conf[i] = d.conf[i] + h * d.dcdt[i];
+  d.conf[Np + i] = d.conf[Np + i] + h * d.dcdt[Np + i];
+  d.conf[2 * Np + i] = d.conf[2 * Np + i] + h * d.dcdt[2 * Np + i];
+  if (p.dim == 3) {
+    v.z = v.z + hm * d.f[2 * Np + i];
+    d.conf[3 * Np + i] = d.conf[3 * Np + i] + h * d.dcdt[3 * Np + i];
+    d.conf[4 * Np + i] = d.conf[4 * Np + i] + h * d.dcdt[4 * Np + i];
+    d.conf[5 * Np + i] = d.conf[5 * Np + i] + h * d.dcdt[5 * Np + i];
+  }
+  d.vel[i] = v;
+}
+
+// Hamilton product (kernel_quaternion_product.cu:15-31)
+__device__ __forceinline__ void qmul(const double* c, const double* e, double* r) {
+  r[0] = c[0] * e[0] - c[1] * e[1] - c[2] * e[2] - c[3] * e[3];
+  r[1] = c[0] * e[1] + c[1] * e[0] + c[2] * e[3] - c[3] * e[2];
+  r[2] = c[0] * e[2] - c[1] * e[3] + c[2] * e[0] + c[3] * e[1];
+  r[3] = c[0] * e[3] + c[1] * e[2] - c[2] * e[1] + c[3] * e[0];
+}
+
+// Rigid colloid half-kick, drift, rotation and re-placement of its boundary particles
+// (kernel_move_colloids_VV_part1.cu:15-204).  One block per colloid.
+__global__ void k_vv1_colloids(Dev d) {
+  const int c = blockIdx.x;
+  if (c >= d.ncoll) return;
+  const BoxParams& p = d.box[d.coll_box[c]];
+  if (p.coll_move != 0) return;
+  __shared__ double rot[4];  // 2D: cos, sin; 3D: quaternion
+  __shared__ double ctr[3];
+  const int nc = d.ncoll;
+  double* cs = d.cs;
+  const double dt = p.dt;
+  if (threadIdx.x == 0) {
+    double hm = 0.5 * dt / p.coll_mass, hI = 0.5 * dt / p.coll_I;
+    double cx = cs[CS_X * nc + c], cy = cs[CS_Y * nc + c], cz = cs[CS_Z * nc + c];
+    cs[CS_VX * nc + c] += hm * cs[CS_FX * nc + c];
+    cs[CS_VY * nc + c] += hm * cs[CS_FY * nc + c];
+    if (p.dim == 3) cs[CS_VZ * nc + c] += hm * cs[CS_FZ * nc + c];
+    cs[CS_OZ * nc + c] += hI * cs[CS_TZ * nc + c];
+    double omega;
+    if (p.dim == 2) {
+      omega = cs[CS_OZ * nc + c];
+    } else {
+      cs[CS_OX * nc + c] += hI * cs[CS_TX * nc + c];
+      cs[CS_OY * nc + c] += hI * cs[CS_TY * nc + c];
+      double ox = cs[CS_OX * nc + c], oy = cs[CS_OY * nc + c], oz = cs[CS_OZ * nc + c];
+      omega = sqrt(ox * ox + oy * oy + oz * oz);
+    }
+    cx = cx + cs[CS_VX * nc + c] * dt;
+    cy = cy + cs[CS_VY * nc + c] * dt;
+    if (p.dim == 3) cz = cz + cs[CS_VZ * nc + c] * dt;
+    if (cx < 0) cx = cx + p.L[0];
+    if (cx > p.L[0]) cx = cx - p.L[0];
+    if (p.wall == 0) {
+      if (cy < 0) cy = cy + p.L[1];
+      if (cy > p.L[1]) cy = cy - p.L[1];
+    }
+    if (p.dim == 3) {
+      if (cz < 0) cz = cz + p.L[2];
+      if (cz > p.L[2]) cz = cz - p.L[2];
+    }
+    cs[CS_X * nc + c] = cx;
+    cs[CS_Y * nc + c] = cy;
+    if (p.dim == 3) cs[CS_Z * nc + c] = cz;
+    ctr[0] = cx;
+    ctr[1] = cy;
+    ctr[2] = cz;
+    if (p.dim == 2) {
+      double th = cs[CS_THETA * nc + c] + cs[CS_OZ * nc + c] * dt;
+      rot[1] = sin(th);
+      rot[0] = cos(th);
+      cs[CS_THETA * nc + c] = th;
+    } else {
+      // omega = 0 gives a NaN axis, as in the reference (:123-125); the NaN positions are
+      // then reported as SPH_ERR_NAN by the hash instead of trapping.
+      double half = 0.5 * omega * dt;
+      double ax = cs[CS_OX * nc + c] / omega, ay = cs[CS_OY * nc + c] / omega,
+             az = cs[CS_OZ * nc + c] / omega;
+      double sh = sin(half);
+      double dq[4] = {cos(half), sh * ax, sh * ay, sh * az};
+      double q[4] = {cs[CS_Q0 * nc + c], cs[CS_QX * nc + c], cs[CS_QY * nc + c],
+                     cs[CS_QZ * nc + c]};
+      double r[4];
+      qmul(dq, q, r);
+      cs[CS_Q0 * nc + c] = r[0];
+      cs[CS_QX * nc + c] = r[1];
+      cs[CS_QY * nc + c] = r[2];
+      cs[CS_QZ * nc + c] = r[3];
+      rot[0] = r[0];
+      rot[1] = r[1];
+      rot[2] = r[2];
+      rot[3] = r[3];
+    }
+  }
+  __syncthreads();
+  const int j0 = d.coll_seg[c], j1 = d.coll_seg[c + 1];
+  const int NL = d.Nlist_coll;
+  for (int j = j0 + threadIdx.x; j < j1; j += blockDim.x) {
+    const int slot = d.inv[d.colloids_list[j]];
+    double px, py, pz = 0.0;
+    if (p.dim == 2) {
+      double x0 = d.xc[j], y0 = d.xc[NL + j];
+      px = x0 * rot[0] - y0 * rot[1];
+      py = x0 * rot[1] + y0 * rot[0];
+    } else {
+      double q[4] = {rot[0], rot[1], rot[2], rot[3]};
+      double qi[4] = {rot[0], -rot[1], -rot[2], -rot[3]};
+      double pt[4] = {0.0, d.xc[j], d.xc[NL + j], d.xc[2 * NL + j]};
+      double t1[4], t2[4];
+      qmul(q, pt, t1);
+      qmul(t1, qi, t2);
+      px = t2[1];
+      py = t2[2];
+      pz = t2[3];
+    }
+    double4 x = d.pos[slot];
+    x.x = px + ctr[0];
+    x.y = py + ctr[1];
+    if (p.dim == 3) x.z = pz + ctr[2];
+    if (x.x < 0) x.x = x.x + p.L[0];
+    if (x.x > p.L[0]) x.x = x.x - p.L[0];
+    if (p.wall == 0) {
+      if (x.y < 0) x.y = x.y + p.L[1];
+      if (x.y > p.L[1]) x.y = x.y - p.L[1];
+    }
+    if (p.dim == 3) {
+      if (x.z < 0) x.z = x.z + p.L[2];
+      if (x.z > p.L[2]) x.z = x.z - p.L[2];
+    }
+    d.pos[slot] = x;
+  }
+}
+
+// kernel_move_colloids_VV_part2.cu:14-46
+__global__ void k_vv2_colloids(Dev d) {
+  int c = blockIdx.x * blockDim.x + threadIdx.x;
+  if (c >= d.ncoll) return;
+  const BoxParams& p = d.box[d.coll_box[c]];
+  if (p.coll_move != 0) return;
+  const int nc = d.ncoll;
+  double* cs = d.cs;
+  double hm = 0.5 * p.dt / p.coll_mass, hI = 0.5 * p.dt / p.coll_I;
+  cs[CS_VX * nc + c] += hm * cs[CS_FX * nc + c];
+  cs[CS_VY * nc + c] += hm * cs[CS_FY * nc + c];
+  if (p.dim == 3) cs[CS_VZ * nc + c] += hm * cs[CS_FZ * nc + c];
+  cs[CS_OZ * nc + c] += hI * cs[CS_TZ * nc + c];
+  if (p.dim == 3) {
+    cs[CS_OX * nc + c] += hI * cs[CS_TX * nc + c];
+    cs[CS_OY * nc + c] += hI * cs[CS_TY * nc + c];
+  }
+}
+
+// ---------------------------------------------------------------------------------
+// Neighbour search: hash -> (radix sort, sph_sort.cu) -> reorder + cell ranges -> lists
+// ---------------------------------------------------------------------------------
+__global__ void k_hash(Dev d) {
+  int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= d.Ntot) return;
+  int ti = d.tinfo[i];
+  const BoxParams& p = d.box[box_of(ti)];
+  double4 x = d.pos[i];
+  int c = hash_cell(p, x.x, x.y, x.z);
+  if (c < 0) {
+    raise_status(d, c == -2 ? kStatNaN : kStatCellRange, d.gid[i]);
+    c = 0;  // keep the sort in bounds; the step is reported as failed
+  }
+  d.key_by_gid[d.gid[i]] = p.cell0 + c;
+}
+
+// Gathers the state into the new slot order and records the cell ranges.
+// cell_begin (dense, all cells) drives the engine; cell_start / cell_end keep the
+// reference's semantics: written for occupied cells only, box-local slot numbers
+// (kernel_cell_ranges.cu:13-33).
+template <bool MIXED, bool PERMUTE_F>
+__global__ void k_reorder(Dev d) {
+  int k = blockIdx.x * blockDim.x + threadIdx.x;
+  if (k >= d.Ntot) return;
+  const int g = d.vals[k];
+  const int o = d.inv[g];
+  const int Np = d.Npad;
+  double4 x = d.pos[o];
+  d.pos_b[k] = x;
+  d.vel_b[k] = d.vel[o];
+#pragma unroll
+  for (int q = 0; q < 6; ++q) d.conf_b[q * Np + k] = d.conf[q * Np + o];
+  if (PERMUTE_F) {
+#pragma unroll
+    for (int q = 0; q < 3; ++q) d.f_b[q * Np + k] = d.f[q * Np + o];
+#pragma unroll
+    for (int q = 0; q < 6; ++q) d.dcdt_b[q * Np + k] = d.dcdt[q * Np + o];
+  }
+  int ti = d.tinfo[o];
+  d.tinfo_b[k] = ti;
+  d.gid_b[k] = g;
+  d.inv[g] = k;
+  if (MIXED) d.pos_f[k] = make_float4((float)x.x, (float)x.y, (float)x.z, (float)x.w);
+  const int key = d.keys[k];
+  const int prev = k > 0 ? d.keys[k - 1] : -1;
+  for (int c = prev + 1; c <= key; ++c) d.cell_begin[c] = k;
+  if (k == d.Ntot - 1)
+    for (int c = key + 1; c <= d.Ctot; ++c) d.cell_begin[c] = d.Ntot;
+  const int slot0 = d.box[box_of(ti)].slot0;
+  if (k == 0 || prev != key) d.cell_start[key] = k - slot0;
+  if (k == d.Ntot - 1 || d.keys[k + 1] != key) d.cell_end[key] = k - slot0;
+}
+
+// One warp per cell: the cell's particles (<= 32 per round) test the candidates of the
+// 3^d neighbour cells, staged 32 at a time in shared memory as float offsets from the
+// cell corner, and append hits to their own lists.  Candidate ranges come from the
+// reference-semantics cell_start / cell_end, so the candidate set and order are the
+// reference's (kernel_densities.cu:52-163), stale ranges included.  The float test uses
+// a slightly enlarged cutoff; consumers apply the exact test.  A particle whose own
+// (unclamped) cell differs from its sort cell (x exactly at L) is listed separately
+// with its own neighbour cells.
+constexpr int kListWarps = 8;
+
+template <int DIM>
+__global__ void __launch_bounds__(kListWarps * 32) k_build_lists(Dev d) {
+  __shared__ float4 stage[kListWarps][32];
+  const int w = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const int cell = blockIdx.x * kListWarps + w;
+  if (cell >= d.Ctot) return;
+  const int b = d.cell_box[cell];
+  const BoxParams& p = d.box[b];
+  const int N0 = p.Ncells[0], N1 = p.Ncells[1], N2 = p.Ncells[2];
+  const int lc = cell - p.cell0;
+  const int cx = lc % N0, cy = (lc / N0) % N1, cz = DIM == 3 ? lc / (N0 * N1) : 0;
+  const int beg = d.cell_begin[cell], end = d.cell_begin[cell + 1];
+  const double ox = cx * p.cell_size[0];
+  const double oy = cy * p.cell_size[1] - (p.wall ? p.wall_width : 0.0);
+  const double oz = DIM == 3 ? cz * p.cell_size[2] : 0.0;
+  const float cut2 = (float)p.list_cut2;
+  const int cap = d.cap, Np = d.Npad;
+  int maxcnt = 0;
+  for (int t0 = beg; t0 < end; t0 += 32) {
+    const int i = t0 + lane;
+    const bool active = i < end;
+    float xi = 0.f, yi = 0.f, zi = 0.f;
+    bool odd = false;
+    if (active) {
+      double4 x = d.pos[i];
+      xi = (float)(x.x - ox);
+      yi = (float)(x.y - oy);
+      zi = (float)(x.z - oz);
+      int ax, ay, az;
+      own_cell(p, x.x, x.y, x.z, ax, ay, az);
+      odd = (ax != cx) || (ay != cy) || (DIM == 3 && az != cz);
+    }
+    int cnt = 0;
+    for (int ddx = -1; ddx <= 1; ++ddx)
+      for (int ddy = -1; ddy <= 1; ++ddy)
+        for (int ddz = (DIM == 3 ? -1 : 0); ddz <= (DIM == 3 ? 1 : 0); ++ddz) {
+          int nx = cx + ddx, ny = cy + ddy, nz = cz + ddz;
+          double sx = 0.0, sy = 0.0, sz = 0.0;
+          if (nx < 0) { nx += N0; sx = -p.L[0]; }
+          if (nx >= N0) { nx -= N0; sx = p.L[0]; }
+          if (DIM == 3) {
+            if (nz < 0) { nz += N2; sz = -p.L[2]; }
+            if (nz >= N2) { nz -= N2; sz = p.L[2]; }
+          }
+          if (!p.wall) {
+            if (ny < 0) { ny += N1; sy = -p.L[1]; }
+            if (ny >= N1) { ny -= N1; sy = p.L[1]; }
+          }
+          if (ny < 0 || ny >= N1) continue;
+          const int nc = p.cell0 + (DIM == 3 ? (nz * N1 + ny) * N0 + nx : ny * N0 + nx);
+          const int s = d.cell_start[nc] + p.slot0, e = d.cell_end[nc] + p.slot0;
+          for (int c0 = s; c0 <= e; c0 += 32) {
+            const int j = c0 + lane;
+            if (j <= e) {
+              double4 xj = d.pos[j];
+              stage[w][lane] = make_float4((float)(xj.x + sx - ox), (float)(xj.y + sy - oy),
+                                           (float)(xj.z + sz - oz), __int_as_float(j));
+            }
+            __syncwarp();
+            const int n = min(32, e - c0 + 1);
+            if (active && !odd) {
+              for (int q = 0; q < n; ++q) {
+                const float4 c = stage[w][q];
+                const float rx = xi - c.x, ry = yi - c.y;
+                float r2 = rx * rx + ry * ry;
+                if (DIM == 3) {
+                  const float rz = zi - c.z;
+                  r2 += rz * rz;
+                }
+                if (r2 < cut2) {
+                  if (cnt < cap) d.nbr[(size_t)cnt * Np + i] = __float_as_int(c.w);
+                  ++cnt;
+                }
+              }
+            }
+            __syncwarp();
+          }
+        }
+    if (active && !odd) {
+      d.nbr_cnt[i] = cnt;
+      maxcnt = max(maxcnt, cnt);
+    }
+    // particles exactly on the upper box edge: their own neighbour cells
+    unsigned odd_mask = __ballot_sync(SPH_FULL, active && odd);
+    while (odd_mask) {
+      const int l = __ffs(odd_mask) - 1;
+      odd_mask &= odd_mask - 1;
+      const int ti = t0 + l;
+      const double4 xt = d.pos[ti];
+      int ax, ay, az;
+      own_cell(p, xt.x, xt.y, xt.z, ax, ay, az);
+      const double tox = ax * p.cell_size[0];
+      const double toy = ay * p.cell_size[1] - (p.wall ? p.wall_width : 0.0);
+      const double toz = DIM == 3 ? az * p.cell_size[2] : 0.0;
+      const float txi = (float)(xt.x - tox), tyi = (float)(xt.y - toy), tzi = (float)(xt.z - toz);
+      int tcnt = 0;
+      for (int ddx = -1; ddx <= 1; ++ddx)
+        for (int ddy = -1; ddy <= 1; ++ddy)
+          for (int ddz = (DIM == 3 ? -1 : 0); ddz <= (DIM == 3 ? 1 : 0); ++ddz) {
+            int nx = ax + ddx, ny = ay + ddy, nz = az + ddz;
+            double sx = 0.0, sy = 0.0, sz = 0.0;
+            if (nx < 0) { nx += N0; sx = -p.L[0]; }
+            if (nx >= N0) { nx -= N0; sx = p.L[0]; }
+            if (DIM == 3) {
+              if (nz < 0) { nz += N2; sz = -p.L[2]; }
+              if (nz >= N2) { nz -= N2; sz = p.L[2]; }
+            }
+            if (!p.wall) {
+              if (ny < 0) { ny += N1; sy = -p.L[1]; }
+              if (ny >= N1) { ny -= N1; sy = p.L[1]; }
+            }
+            if (ny < 0 || ny >= N1) continue;
+            const int nc = p.cell0 + (DIM == 3 ? (nz * N1 + ny) * N0 + nx : ny * N0 + nx);
+            const int s = d.cell_start[nc] + p.slot0, e = d.cell_end[nc] + p.slot0;
+            for (int c0 = s; c0 <= e; c0 += 32) {
+              const int j = c0 + lane;
+              bool hit = false;
+              if (j <= e) {
+                double4 xj = d.pos[j];
+                const float rx = txi - (float)(xj.x + sx - tox);
+                const float ry = tyi - (float)(xj.y + sy - toy);
+                float r2 = rx * rx + ry * ry;
+                if (DIM == 3) {
+                  const float rz = tzi - (float)(xj.z + sz - toz);
+                  r2 += rz * rz;
+                }
+                hit = r2 < cut2;
+              }
+              const unsigned hits = __ballot_sync(SPH_FULL, hit);
+              const int pos = tcnt + __popc(hits & ((1u << lane) - 1u));
+              if (hit && pos < cap) d.nbr[(size_t)pos * Np + ti] = j;
+              tcnt += __popc(hits);
+            }
+          }
+      if (lane == 0) d.nbr_cnt[ti] = tcnt;
+      maxcnt = max(maxcnt, tcnt);
+    }
+  }
+  // warp max of the counts -> capacity check
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) maxcnt = max(maxcnt, __shfl_xor_sync(SPH_FULL, maxcnt, o));
+  if (lane == 0 && maxcnt > 0) {
+    atomicMax(&d.err_info[1], maxcnt);
+    if (maxcnt > cap) atomicOr(d.status, (unsigned)kStatCapacity);
+  }
+}
+
+// Colloid coarse grid (kernel_cell_colloids_list.cu, kernel_initialize_cell_colloids.cu,
+// kernel_cell_colloids_ranges.cu) with the stable (cell, index) order of thrust's sort.
+// One block per box.
+__global__ void k_colloid_cells(Dev d, int nboxes) {
+  const int b = blockIdx.x;
+  if (b >= nboxes) return;
+  const BoxParams& p = d.box[b];
+  const int n = p.N_colloids;
+  if (n < 2) return;
+  const int c0 = p.coll0, nc = d.ncoll;
+  extern __shared__ int s_cell[];
+  for (int i = threadIdx.x; i < n; i += blockDim.x) {
+    double x = d.cs[CS_X * nc + c0 + i], y = d.cs[CS_Y * nc + c0 + i];
+    int cx = (int)floor(x / p.cell_colloids_size[0]);
+    int cy = (int)floor(y / p.cell_colloids_size[1]);
+    int c;
+    if (p.dim == 3) {
+      int cz = (int)floor(d.cs[CS_Z * nc + c0 + i] / p.cell_colloids_size[2]);
+      c = cz * p.Ncells_colloids[0] * p.Ncells_colloids[1] + cy * p.Ncells_colloids[0] + cx;
+    } else {
+      c = cy * p.Ncells_colloids[0] + cx;
+    }
+    s_cell[i] = c;
+  }
+  for (int c = threadIdx.x; c < p.Ntotal_cells_colloids; c += blockDim.x) {
+    d.ccell_start[p.ccell0 + c] = -1;
+    d.ccell_end[p.ccell0 + c] = -2;
+  }
+  __syncthreads();
+  for (int i = threadIdx.x; i < n; i += blockDim.x) {
+    const int ci = s_cell[i];
+    int rank = 0;
+    for (int j = 0; j < n; ++j) rank += (s_cell[j] < ci) || (s_cell[j] == ci && j < i);
+    d.ccell[c0 + rank] = ci;
+    d.cindex[c0 + rank] = i;
+  }
+  __syncthreads();
+  for (int i = threadIdx.x; i < n; i += blockDim.x) {
+    const int ci = d.ccell[c0 + i];
+    if (ci < 0 || ci >= p.Ntotal_cells_colloids) continue;
+    if (i == 0 || d.ccell[c0 + i - 1] != ci) d.ccell_start[p.ccell0 + ci] = i;
+    if (i == n - 1 || d.ccell[c0 + i + 1] != ci) d.ccell_end[p.ccell0 + ci] = i;
+  }
+}
+
+// ---------------------------------------------------------------------------------
+// Density (kernel_densities.cu:16-193) over the neighbour list, with the pressure
+// (kernel_pressures.cu:13-23) and the neighbour record of the particle as epilogue.
+// ---------------------------------------------------------------------------------
+template <typename T>
+__device__ __forceinline__ void write_record(const Dev& d, int i, const BoxParams& p, int ti,
+                                             double dens, double press) {
+  using Rec = typename RecOf<T>::type;
+  Rec* rec = reinterpret_cast<Rec*>(d.rec);
+  const int Np = d.Npad;
+  const double4 x = d.pos[i];
+  const double4 v = d.vel[i];
+  Rec r;
+  r.x = x.x; r.y = x.y; r.z = x.z;
+  r.vx = v.x; r.vy = v.y; r.vz = v.z;
+  const double nkT = p.nkT;
+  double c[6];
+#pragma unroll
+  for (int q = 0; q < 6; ++q) c[q] = d.conf[q * Np + i];
+  const double dinv = 1.0 / dens;
+  if (type_of(ti) == 0) {
+    // Pi / d^2 with Pi = p I - nkT c (kernel_forces.cu:62-88)
+    const double dsq = dinv * dinv;
+    r.P[0] = (T)((press - nkT * c[0]) * dsq);
+    r.P[1] = (T)((-nkT * c[1]) * dsq);
+    r.P[2] = (T)((press - nkT * c[2]) * dsq);
+    r.P[3] = (T)((-nkT * c[3]) * dsq);
+    r.P[4] = (T)((-nkT * c[4]) * dsq);
+    r.P[5] = (T)((press - nkT * c[5]) * dsq);
+  } else {
+    // walls / colloid particles: -nkT c, completed with the fluid partner's p and d
+#pragma unroll
+    for (int q = 0; q < 6; ++q) r.P[q] = (T)(-nkT * c[q]);
+  }
+  r.invd = (T)dinv;
+  r.tinfo = ti;
+  rec[i] = r;
+}
+
+template <typename T, int DIM>
+__global__ void k_density(Dev d) {
+  using V = typename V4<T>::type;
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= d.Ntot) return;
+  // positions: the double state itself, or its float copy in mixed precision
+  const V* __restrict__ P = sizeof(T) == 8 ? reinterpret_cast<const V*>(d.pos)
+                                           : reinterpret_cast<const V*>(d.pos_f);
+  const int ti = d.tinfo[i];
+  const BoxParams& p = d.box[box_of(ti)];
+  const T L[3] = {(T)p.L[0], (T)p.L[1], (T)p.L[2]};
+  const T h[3] = {(T)p.halfL[0], (T)p.halfL[1], (T)p.halfL[2]};
+  const T rcutsq = (T)p.rcutsq;
+  const T rcut_inv = (T)p.rcut_inv, cw = (T)p.cw;
+  const V xi = P[i];
+  const int n = min(d.nbr_cnt[i], d.cap);
+  const int Np = d.Npad;
+  T dens = T(0);
+  for (int k = 0; k < n; ++k) {
+    const int j = __ldg(&d.nbr[(size_t)k * Np + i]);
+    const V xj = P[j];
+    T rx = xi.x - xj.x, ry = xi.y - xj.y, rz = DIM == 3 ? xi.z - xj.z : T(0);
+    min_image<T, DIM>(rx, ry, rz, L, h, p.wall);
+    const T r2 = DIM == 3 ? rx * rx + ry * ry + rz * rz : rx * rx + ry * ry;
+    if (r2 < rcutsq) dens = dens + sph_w<T>(sqrt(r2), rcut_inv, cw);
+  }
+  const double densd = (double)dens;
+  d.dens[i] = densd;
+  const double press = p.csq * (d.pos[i].w * densd - p.rho0);
+  d.press[i] = press;
+  write_record<T>(d, i, p, ti, densd, press);
+}
+
+// kernel_pressures.cu:13-23 (standalone, also refreshes the neighbour record)
+template <typename T>
+__global__ void k_pressure(Dev d) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= d.Ntot) return;
+  const int ti = d.tinfo[i];
+  const BoxParams& p = d.box[box_of(ti)];
+  const double dens = d.dens[i];
+  const double press = p.csq * (d.pos[i].w * dens - p.rho0);
+  d.press[i] = press;
+  write_record<T>(d, i, p, ti, dens, press);
+}
+
+// ---------------------------------------------------------------------------------
+// Pair pass: velocity gradient (kernel_vel_gradients.cu:15-662), forces
+// (kernel_forces.cu:15-865), external force (kernel_ext_force.cu:13-73) and dc/dt
+// (kernel_dcdt.cu:15-104) for each particle, from its neighbour list.
+// ---------------------------------------------------------------------------------
+struct CollView {
+  const double* cs;
+  int nc;
+};
+
+// Morris ghost velocity, fluid particle i next to wall / colloid particle j
+// (kernel_forces.cu:234-318, 590-692; kernel_vel_gradients.cu:162-247, 421-525).
+template <typename T, int DIM>
+__device__ __forceinline__ void ghost_fluid_i(const BoxParams& p, const CollView& cv,
+                                              int tj, int coll0, T xi, T yi, T zi, T yj,
+                                              const T vi[3], const T r[3], const T L[3],
+                                              const T h[3], T v[3]) {
+  const T beta_max = (T)p.beta_max;
+  if (tj == 1 || tj == 2) {
+    T di, dj, Vw;
+    if (tj == 1) {
+      di = yi - (T)p.y_bottom;
+      dj = (T)p.y_bottom - yj;
+      Vw = (T)p.V_bottom;
+    } else {
+      di = (T)p.y_top - yi;
+      dj = yj - (T)p.y_top;
+      Vw = (T)p.V_top;
+    }
+    T beta = T(1) + dj / di;
+    if (beta > beta_max) beta = beta_max;
+    if (di > T(0)) {
+      v[0] = beta * (vi[0] - Vw);
+      v[1] = beta * vi[1];
+      v[2] = beta * vi[2];
+    } else {
+      v[0] = vi[0] - Vw;
+      v[1] = vi[1];
+      v[2] = vi[2];
+    }
+    return;
+  }
+  const int c = coll0 + tj - 3, nc = cv.nc;
+  T rc[3] = {xi - (T)cv.cs[CS_X * nc + c], yi - (T)cv.cs[CS_Y * nc + c],
+             DIM == 3 ? zi - (T)cv.cs[CS_Z * nc + c] : T(0)};
+  min_image<T, DIM>(rc[0], rc[1], rc[2], L, h, p.wall);
+  const T dc = DIM == 3 ? sqrt(rc[0] * rc[0] + rc[1] * rc[1] + rc[2] * rc[2])
+                        : sqrt(rc[0] * rc[0] + rc[1] * rc[1]);
+  const T R = (T)p.coll_R;
+  const T dis = dc - R;
+  const T cvel[3] = {(T)cv.cs[CS_VX * nc + c], (T)cv.cs[CS_VY * nc + c],
+                     DIM == 3 ? (T)cv.cs[CS_VZ * nc + c] : T(0)};
+  if (dis < T(0)) {
+    v[0] = vi[0] - cvel[0];
+    v[1] = vi[1] - cvel[1];
+    v[2] = vi[2] - cvel[2];
+    return;
+  }
+  const T xs = rc[0] / dc * R, ys = rc[1] / dc * R, zs = DIM == 3 ? rc[2] / dc * R : T(0);
+  T vr[3];
+  const T wz = (T)cv.cs[CS_OZ * nc + c];
+  if (DIM == 2) {
+    vr[0] = -wz * ys;
+    vr[1] = wz * xs;
+    vr[2] = T(0);
+  } else {
+    const T wx = (T)cv.cs[CS_OX * nc + c], wy = (T)cv.cs[CS_OY * nc + c];
+    vr[0] = wy * zs - wz * ys;
+    vr[1] = wz * xs - wx * zs;
+    vr[2] = wx * ys - wy * xs;
+  }
+  const T sv0 = rc[0] / dc, sv1 = rc[1] / dc, sv2 = DIM == 3 ? rc[2] / dc : T(0);
+  const T djs = DIM == 3 ? (r[0] * sv0 + r[1] * sv1 + r[2] * sv2) - dis
+                         : (r[0] * sv0 + r[1] * sv1) - dis;
+  T beta = T(1) + djs / dis;
+  if (beta > beta_max) beta = beta_max;
+  v[0] = beta * (vi[0] - cvel[0] - vr[0]);
+  v[1] = beta * (vi[1] - cvel[1] - vr[1]);
+  v[2] = beta * (vi[2] - cvel[2] - vr[2]);
+}
+
+// Morris ghost velocity, wall / colloid particle i next to particle j
+// (kernel_forces.cu:337-418, 721-821; kernel_vel_gradients.cu:249-331, 527-630).
+template <typename T, int DIM>
+__device__ __forceinline__ void ghost_solid_i(const BoxParams& p, const CollView& cv,
+                                              int ti, int coll0, T yi, T xj, T yj, T zj,
+                                              const T vj[3], const T r[3], const T L[3],
+                                              const T h[3], T v[3]) {
+  const T beta_max = (T)p.beta_max;
+  if (ti == 1 || ti == 2) {
+    T di, dj, Vw;
+    if (ti == 1) {
+      di = (T)p.y_bottom - yi;
+      dj = yj - (T)p.y_bottom;
+      Vw = (T)p.V_bottom;
+    } else {
+      di = yi - (T)p.y_top;
+      dj = (T)p.y_top - yj;
+      Vw = (T)p.V_top;
+    }
+    T beta = T(1) + di / dj;
+    if (beta > beta_max) beta = beta_max;
+    if (dj > T(0)) {
+      v[0] = beta * (Vw - vj[0]);
+      v[1] = -beta * vj[1];
+      v[2] = -beta * vj[2];
+    } else {
+      v[0] = Vw - vj[0];
+      v[1] = -vj[1];
+      v[2] = -vj[2];
+    }
+    return;
+  }
+  const int c = coll0 + ti - 3, nc = cv.nc;
+  T rc[3] = {xj - (T)cv.cs[CS_X * nc + c], yj - (T)cv.cs[CS_Y * nc + c],
+             DIM == 3 ? zj - (T)cv.cs[CS_Z * nc + c] : T(0)};
+  min_image<T, DIM>(rc[0], rc[1], rc[2], L, h, p.wall);
+  const T dc = DIM == 3 ? sqrt(rc[0] * rc[0] + rc[1] * rc[1] + rc[2] * rc[2])
+                        : sqrt(rc[0] * rc[0] + rc[1] * rc[1]);
+  const T R = (T)p.coll_R;
+  const T djs = dc - R;
+  const T cvel[3] = {(T)cv.cs[CS_VX * nc + c], (T)cv.cs[CS_VY * nc + c],
+                     DIM == 3 ? (T)cv.cs[CS_VZ * nc + c] : T(0)};
+  if (djs < T(0)) {
+    v[0] = cvel[0] - vj[0];
+    v[1] = cvel[1] - vj[1];
+    v[2] = cvel[2] - vj[2];
+    return;
+  }
+  const T xs = rc[0] / dc * R, ys = rc[1] / dc * R, zs = DIM == 3 ? rc[2] / dc * R : T(0);
+  T vr[3];
+  const T wz = (T)cv.cs[CS_OZ * nc + c];
+  if (DIM == 2) {
+    vr[0] = -wz * ys;
+    vr[1] = wz * xs;
+    vr[2] = T(0);
+  } else {
+    const T wx = (T)cv.cs[CS_OX * nc + c], wy = (T)cv.cs[CS_OY * nc + c];
+    vr[0] = wy * zs - wz * ys;
+    vr[1] = wz * xs - wx * zs;
+    vr[2] = wx * ys - wy * xs;
+  }
+  const T sv0 = rc[0] / dc, sv1 = rc[1] / dc, sv2 = DIM == 3 ? rc[2] / dc : T(0);
+  const T dis = DIM == 3 ? (-r[0] * sv0 - r[1] * sv1 - r[2] * sv2) - djs
+                         : (-r[0] * sv0 - r[1] * sv1) - djs;
+  T beta = T(1) + dis / djs;
+  if (beta > beta_max) beta = beta_max;
+  v[0] = beta * (cvel[0] + vr[0] - vj[0]);
+  v[1] = beta * (cvel[1] + vr[1] - vj[1]);
+  v[2] = beta * (cvel[2] + vr[2] - vj[2]);
+}
+
+template <typename T, int DIM, int MODE, bool EXT>
+__global__ void __launch_bounds__(128) k_pairs(Dev d) {
+  using Rec = typename RecOf<T>::type;
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= d.Ntot) return;
+  const Rec* __restrict__ rec = reinterpret_cast<const Rec*>(d.rec);
+  const int tinfo_i = d.tinfo[i];
+  const int ti = type_of(tinfo_i);
+  const BoxParams& p = d.box[box_of(tinfo_i)];
+  const T L[3] = {(T)p.L[0], (T)p.L[1], (T)p.L[2]};
+  const T h[3] = {(T)p.halfL[0], (T)p.halfL[1], (T)p.halfL[2]};
+  const T rcutsq = (T)p.rcutsq, rcut_inv = (T)p.rcut_inv, c_gradw = (T)p.c_gradw;
+  const T ca = (T)p.a, cb = (T)p.b;
+  const CollView cv{d.cs, d.ncoll};
+  const int coll0 = p.coll0;
+  const Rec ri = rec[i];
+  const T xi = (T)ri.x, yi = (T)ri.y, zi = (T)ri.z;
+  const T vi[3] = {(T)ri.vx, (T)ri.vy, DIM == 3 ? (T)ri.vz : T(0)};
+  const T invd_i = ri.invd;
+  const T press_i = (T)d.press[i];
+  T Pi0[6];
+#pragma unroll
+  for (int q = 0; q < 6; ++q) Pi0[q] = ri.P[q];
+  const bool fluid_i = ti == 0;
+  // gradient: fluid particles in the fused pass, every particle in kPairGradvAll
+  const bool do_grad = (MODE == kPairGradvAll) || (MODE == kPairFused && fluid_i);
+  const bool do_force = MODE != kPairGradvAll;
+  T g[DIM][DIM];
+#pragma unroll
+  for (int a = 0; a < DIM; ++a)
+#pragma unroll
+    for (int c = 0; c < DIM; ++c) g[a][c] = T(0);
+  T f[3] = {T(0), T(0), T(0)};
+  const int n = min(d.nbr_cnt[i], d.cap);
+  const int Np = d.Npad;
+  for (int k = 0; k < n; ++k) {
+    const int j = __ldg(&d.nbr[(size_t)k * Np + i]);
+    if (j == i) continue;
+    const Rec rj = rec[j];
+    const int tj = type_of(rj.tinfo);
+    const bool fluid_j = tj == 0;
+    // skip rules: gradient kernel_vel_gradients.cu:126-127, forces kernel_forces.cu:157-158
+    const bool pair_grad = do_grad && !(ti == tj && !fluid_i);
+    const bool pair_force = do_force && (fluid_i || fluid_j);
+    if (!pair_grad && !pair_force) continue;
+    T r[3] = {xi - (T)rj.x, yi - (T)rj.y, DIM == 3 ? zi - (T)rj.z : T(0)};
+    min_image<T, DIM>(r[0], r[1], r[2], L, h, p.wall);
+    const T r2 = DIM == 3 ? r[0] * r[0] + r[1] * r[1] + r[2] * r[2] : r[0] * r[0] + r[1] * r[1];
+    if (!(r2 < rcutsq)) continue;
+    const T vj[3] = {(T)rj.vx, (T)rj.vy, DIM == 3 ? (T)rj.vz : T(0)};
+    T v[3];
+    if (ti == tj) {
+      v[0] = vi[0] - vj[0];
+      v[1] = vi[1] - vj[1];
+      v[2] = vi[2] - vj[2];
+    } else if (fluid_i) {
+      ghost_fluid_i<T, DIM>(p, cv, tj, coll0, xi, yi, zi, (T)rj.y, vi, r, L, h, v);
+    } else {
+      ghost_solid_i<T, DIM>(p, cv, ti, coll0, yi, (T)rj.x, (T)rj.y, (T)rj.z, vj, r, L, h, v);
+    }
+    const T rr = sqrt(r2);
+    const T rinv = T(1) / rr;
+    const T gw = sph_gradw<T>(rr, rcut_inv, c_gradw);
+    const T e[3] = {r[0] * rinv, r[1] * rinv, DIM == 3 ? r[2] * rinv : T(0)};
+    if (pair_grad) {
+      const T s = -invd_i * gw;
+#pragma unroll
+      for (int a = 0; a < DIM; ++a) {
+        const T se = s * e[a];
+#pragma unroll
+        for (int c = 0; c < DIM; ++c) g[a][c] += se * v[c];
+      }
+    }
+    if (pair_force) {
+      T Pi[6], Pj[6], di, dj;
+      if (fluid_i && fluid_j) {
+#pragma unroll
+        for (int q = 0; q < 6; ++q) {
+          Pi[q] = Pi0[q];
+          Pj[q] = rj.P[q];
+        }
+        di = invd_i;
+        dj = rj.invd;
+      } else if (fluid_i) {
+        // j mirrors i's density and pressure, keeps its own c (kernel_forces.cu:217-233)
+        const T dsq = invd_i * invd_i;
+#pragma unroll
+        for (int q = 0; q < 6; ++q) {
+          Pi[q] = Pi0[q];
+          const T diag = (q == 0 || q == 2 || q == 5) ? press_i : T(0);
+          Pj[q] = (diag + rj.P[q]) * dsq;
+        }
+        di = invd_i;
+        dj = invd_i;
+      } else {
+        // i takes j's density, pressure and c (kernel_forces.cu:320-336)
+#pragma unroll
+        for (int q = 0; q < 6; ++q) {
+          Pj[q] = rj.P[q];
+          Pi[q] = rj.P[q];
+        }
+        di = rj.invd;
+        dj = rj.invd;
+      }
+      const T axx = -gw * (Pi[0] + Pj[0]);
+      const T axy = -gw * (Pi[1] + Pj[1]);
+      const T ayy = -gw * (Pi[2] + Pj[2]);
+      const T aux = gw * di * dj * rinv;
+      const T aux1 = ca * aux;
+      if (DIM == 2) {
+        const T ev = e[0] * v[0] + e[1] * v[1];
+        f[0] += axx * e[0] + axy * e[1];
+        f[1] += axy * e[0] + ayy * e[1];
+        const T aux2 = cb * aux * ev;
+        f[0] += aux1 * v[0] + aux2 * e[0];
+        f[1] += aux1 * v[1] + aux2 * e[1];
+      } else {
+        const T axz = -gw * (Pi[3] + Pj[3]);
+        const T ayz = -gw * (Pi[4] + Pj[4]);
+        const T azz = -gw * (Pi[5] + Pj[5]);
+        const T ev = e[0] * v[0] + e[1] * v[1] + e[2] * v[2];
+        f[0] += axx * e[0] + axy * e[1] + axz * e[2];
+        f[1] += axy * e[0] + ayy * e[1] + ayz * e[2];
+        f[2] += axz * e[0] + ayz * e[1] + azz * e[2];
+        const T aux2 = cb * aux * ev;
+        f[0] += aux1 * v[0] + aux2 * e[0];
+        f[1] += aux1 * v[1] + aux2 * e[1];
+        f[2] += aux1 * v[2] + aux2 * e[2];
+      }
+    }
+  }
+  const int Np2 = d.Npad;
+  if (MODE == kPairGradvAll || (MODE == kPairFused && d.gradv != nullptr && do_grad)) {
+    // storage order xx xy xz yx yy yz zx zy zz
+    d.gradv[0 * Np2 + i] = (double)g[0][0];
+    d.gradv[1 * Np2 + i] = (double)g[0][1];
+    d.gradv[3 * Np2 + i] = (double)g[1][0];
+    d.gradv[4 * Np2 + i] = (double)g[1][1];
+    if (DIM == 3) {
+      d.gradv[2 * Np2 + i] = (double)g[0][2];
+      d.gradv[5 * Np2 + i] = (double)g[1][2];
+      d.gradv[6 * Np2 + i] = (double)g[2][0];
+      d.gradv[7 * Np2 + i] = (double)g[2][1];
+      d.gradv[8 * Np2 + i] = (double)g[2][2];
+    }
+  }
+  if (MODE == kPairGradvAll) return;
+  double fx = (double)f[0], fy = (double)f[1], fz = (double)f[2];
+  if (EXT && fluid_i) {
+    const double4 xd = d.pos[i];
+    const double m = xd.w;
+    if (p.ext_force_type == 1) {
+      fx += m * p.ext_force[0];
+      fy += m * p.ext_force[1];
+      if (DIM == 3) fz += m * p.ext_force[2];
+    } else if (p.ext_force_type == 2) {
+      fx += m * p.ext_force[0] * sin(p.ky * xd.y);
+      fy += 0.0;
+      if (DIM == 3) fz += 0.0;
+    } else if (p.ext_force_type == 3) {
+      fx += (xd.y < 0.5 * p.L[1]) ? m * p.ext_force[0] : -(m * p.ext_force[0]);
+      fy += 0.0;
+      if (DIM == 3) fz += 0.0;
+    }
+  }
+  d.f[i] = fx;
+  d.f[Np2 + i] = fy;
+  if (DIM == 3) d.f[2 * Np2 + i] = fz;
+  if (MODE == kPairFused && fluid_i) {
+    // dc/dt = c.g + (c.g)^T + (I - c)/tau  (kernel_dcdt.cu:76-102)
+    const double tinv = 1.0 / p.tau;
+    const double cxx = d.conf[i], cxy = d.conf[Np2 + i], cyy = d.conf[2 * Np2 + i];
+    if (DIM == 2) {
+      const double gxx = g[0][0], gxy = g[0][1], gyx = g[1][0], gyy = g[1][1];
+      const double Axx = cxx * gxx + cxy * gyx, Axy = cxx * gxy + cxy * gyy;
+      const double Ayx = cxy * gxx + cyy * gyx, Ayy = cxy * gxy + cyy * gyy;
+      d.dcdt[i] = 2.0 * Axx + tinv * (1.0 - cxx);
+      d.dcdt[Np2 + i] = Axy + Ayx - tinv * cxy;
+      d.dcdt[2 * Np2 + i] = 2.0 * Ayy + tinv * (1.0 - cyy);
+    } else {
+      const double cxz = d.conf[3 * Np2 + i], cyz = d.conf[4 * Np2 + i], czz = d.conf[5 * Np2 + i];
+      const double gxx = g[0][0], gxy = g[0][1], gxz = g[0][DIM - 1];
+      const double gyx = g[1][0], gyy = g[1][1], gyz = g[1][DIM - 1];
+      const double gzx = g[DIM - 1][0], gzy = g[DIM - 1][1], gzz = g[DIM - 1][DIM - 1];
+      const double Axx = cxx * gxx + cxy * gyx + cxz * gzx;
+      const double Axy = cxx * gxy + cxy * gyy + cxz * gzy;
+      const double Axz = cxx * gxz + cxy * gyz + cxz * gzz;
+      const double Ayx = cxy * gxx + cyy * gyx + cyz * gzx;
+      const double Ayy = cxy * gxy + cyy * gyy + cyz * gzy;
+      const double Ayz = cxy * gxz + cyy * gyz + cyz * gzz;
+      const double Azx = cxz * gxx + cyz * gyx + czz * gzx;
+      const double Azy = cxz * gxy + cyz * gyy + czz * gzy;
+      const double Azz = cxz * gxz + cyz * gyz + czz * gzz;
+      d.dcdt[i] = 2.0 * Axx + tinv * (1.0 - cxx);
+      d.dcdt[Np2 + i] = Axy + Ayx - tinv * cxy;
+      d.dcdt[2 * Np2 + i] = 2.0 * Ayy + tinv * (1.0 - cyy);
+      d.dcdt[3 * Np2 + i] = Axz + Azx - tinv * cxz;
+      d.dcdt[4 * Np2 + i] = Ayz + Azy - tinv * cyz;
+      d.dcdt[5 * Np2 + i] = 2.0 * Azz + tinv * (1.0 - czz);
+    }
+  }
+}
+
+// kernel_ext_force.cu:13-73 as a separate pass (class_system::calculate_external_forces)
+__global__ void k_ext_force(Dev d) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= d.Ntot) return;
+  const int ti = d.tinfo[i];
+  if (type_of(ti) != 0) return;
+  const BoxParams& p = d.box[box_of(ti)];
+  const int Np = d.Npad;
+  const double4 x = d.pos[i];
+  const double m = x.w;
+  if (p.ext_force_type == 1) {
+    d.f[i] += m * p.ext_force[0];
+    d.f[Np + i] += m * p.ext_force[1];
+    if (p.dim == 3) d.f[2 * Np + i] += m * p.ext_force[2];
+  } else if (p.ext_force_type == 2) {
+    d.f[i] += m * p.ext_force[0] * sin(p.ky * x.y);
+    d.f[Np + i] += 0.0;
+    if (p.dim == 3) d.f[2 * Np + i] += 0.0;
+  } else if (p.ext_force_type == 3) {
+    d.f[i] += (x.y < 0.5 * p.L[1]) ? m * p.ext_force[0] : -(m * p.ext_force[0]);
+    d.f[Np + i] += 0.0;
+    if (p.dim == 3) d.f[2 * Np + i] += 0.0;
+  }
+}
+
+// dc/dt from the stored gradient (kernel_dcdt.cu:15-104), used after a standalone
+// velocity-gradient pass.
+__global__ void k_dcdt(Dev d) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= d.Ntot) return;
+  const int ti = d.tinfo[i];
+  if (type_of(ti) != 0) return;
+  const BoxParams& p = d.box[box_of(ti)];
+  const int Np = d.Npad;
+  const double tinv = 1.0 / p.tau;
+  const double* G = d.gradv;
+  const double cxx = d.conf[i], cxy = d.conf[Np + i], cyy = d.conf[2 * Np + i];
+  const double gxx = G[i], gxy = G[Np + i], gyx = G[3 * Np + i], gyy = G[4 * Np + i];
+  if (p.dim == 2) {
+    const double Axx = cxx * gxx + cxy * gyx, Axy = cxx * gxy + cxy * gyy;
+    const double Ayx = cxy * gxx + cyy * gyx, Ayy = cxy * gxy + cyy * gyy;
+    d.dcdt[i] = 2.0 * Axx + tinv * (1.0 - cxx);
+    d.dcdt[Np + i] = Axy + Ayx - tinv * cxy;
+    d.dcdt[2 * Np + i] = 2.0 * Ayy + tinv * (1.0 - cyy);
+    return;
+  }
+  const double cxz = d.conf[3 * Np + i], cyz = d.conf[4 * Np + i], czz = d.conf[5 * Np + i];
+  const double gxz = G[2 * Np + i], gyz = G[5 * Np + i], gzx = G[6 * Np + i],
+               gzy = G[7 * Np + i], gzz = G[8 * Np + i];
+  const double Axx = cxx * gxx + cxy * gyx + cxz * gzx;
+  const double Axy = cxx * gxy + cxy * gyy + cxz * gzy;
+  const double Axz = cxx * gxz + cxy * gyz + cxz * gzz;
+  const double Ayx = cxy * gxx + cyy * gyx + cyz * gzx;
+  const double Ayy = cxy * gxy + cyy * gyy + cyz * gzy;
+  const double Ayz = cxy * gxz + cyy * gyz + cyz * gzz;
+  const double Azx = cxz * gxx + cyz * gyx + czz * gzx;
+  const double Azy = cxz * gxy + cyz * gyy + czz * gzy;
+  const double Azz = cxz * gxz + cyz * gyz + czz * gzz;
+  d.dcdt[i] = 2.0 * Axx + tinv * (1.0 - cxx);
+  d.dcdt[Np + i] = Axy + Ayx - tinv * cxy;
+  d.dcdt[2 * Np + i] = 2.0 * Ayy + tinv * (1.0 - cyy);
+  d.dcdt[3 * Np + i] = Axz + Azx - tinv * cxz;
+  d.dcdt[4 * Np + i] = Ayz + Azy - tinv * cyz;
+  d.dcdt[5 * Np + i] = 2.0 * Azz + tinv * (1.0 - czz);
+}
+
+// ---------------------------------------------------------------------------------
+// Wall forces (kernel_collect_force_walls.cu:15-50) and colloid forces and torques
+// (kernel_collect_force_colloids.cu:15-99): one block per wall / colloid, a fixed-order
+// FP64 tree reduction in place of the reference's one-thread serial loop.
+// ---------------------------------------------------------------------------------
+constexpr int kRedThreads = 256;
+
+template <int NV>
+__device__ __forceinline__ void block_reduce(double (&v)[NV], double (*sh)[kRedThreads]) {
+#pragma unroll
+  for (int q = 0; q < NV; ++q) sh[q][threadIdx.x] = v[q];
+  __syncthreads();
+  for (int s = kRedThreads / 2; s > 0; s >>= 1) {
+    if ((int)threadIdx.x < s)
+#pragma unroll
+      for (int q = 0; q < NV; ++q) sh[q][threadIdx.x] += sh[q][threadIdx.x + s];
+    __syncthreads();
+  }
+#pragma unroll
+  for (int q = 0; q < NV; ++q) v[q] = sh[q][0];
+}
+
+__global__ void __launch_bounds__(kRedThreads) k_wall_forces(Dev d) {
+  __shared__ double sh[3][kRedThreads];
+  const int w = blockIdx.x;
+  if (w >= d.nwallseg) return;
+  const int j0 = d.wall_seg[w], j1 = d.wall_seg[w + 1];
+  const int Np = d.Npad;
+  double v[3] = {0.0, 0.0, 0.0};
+  for (int j = j0 + threadIdx.x; j < j1; j += kRedThreads) {
+    const int s = d.inv[d.walls_list[j]];
+    v[0] += d.f[s];
+    v[1] += d.f[Np + s];
+    v[2] += d.f[2 * Np + s];
+  }
+  block_reduce<3>(v, sh);
+  if (threadIdx.x == 0) {
+    d.wall_f[3 * w + 0] = v[0];
+    d.wall_f[3 * w + 1] = v[1];
+    d.wall_f[3 * w + 2] = v[2];
+  }
+}
+
+__global__ void __launch_bounds__(kRedThreads) k_collect_colloids(Dev d) {
+  __shared__ double sh[6][kRedThreads];
+  const int c = blockIdx.x;
+  if (c >= d.ncoll) return;
+  const BoxParams& p = d.box[d.coll_box[c]];
+  const int nc = d.ncoll, Np = d.Npad;
+  const double cx = d.cs[CS_X * nc + c], cy = d.cs[CS_Y * nc + c], cz = d.cs[CS_Z * nc + c];
+  const int j0 = d.coll_seg[c], j1 = d.coll_seg[c + 1];
+  double v[6] = {0, 0, 0, 0, 0, 0};  // F x y z, T x y z
+  for (int j = j0 + threadIdx.x; j < j1; j += kRedThreads) {
+    const int s = d.inv[d.colloids_list[j]];
+    const double4 x = d.pos[s];
+    const double fx = d.f[s], fy = d.f[Np + s], fz = p.dim == 3 ? d.f[2 * Np + s] : 0.0;
+    double rx = x.x - cx, ry = x.y - cy, rz = 0.0;
+    if (rx > 0.5 * p.L[0]) rx -= p.L[0];
+    if (rx < -0.5 * p.L[0]) rx += p.L[0];
+    if (p.wall == 0) {
+      if (ry > 0.5 * p.L[1]) ry -= p.L[1];
+      if (ry < -0.5 * p.L[1]) ry += p.L[1];
+    }
+    if (p.dim == 3) {
+      rz = x.z - cz;
+      if (rz > 0.5 * p.L[2]) rz -= p.L[2];
+      if (rz < -0.5 * p.L[2]) rz += p.L[2];
+    }
+    v[0] += fx;
+    v[1] += fy;
+    v[2] += fz;
+    v[3] += ry * fz - rz * fy;
+    v[4] += rz * fx - rx * fz;
+    v[5] += rx * fy - ry * fx;
+  }
+  block_reduce<6>(v, sh);
+  if (threadIdx.x == 0) {
+    double* cs = d.cs;
+    cs[CS_FX * nc + c] = v[0];
+    cs[CS_FY * nc + c] = v[1];
+    cs[CS_TZ * nc + c] = v[5];
+    if (p.dim == 3) {
+      cs[CS_FZ * nc + c] = v[2];
+      cs[CS_TX * nc + c] = v[3];
+      cs[CS_TY * nc + c] = v[4];
+    }
+  }
+}
+
+// Colloid-colloid repulsion (kernel_repulsion_force_colloids.cu:21-207, r^2 clamped to the
+// cut-on before normalising) then rotating-field dipole force
+// (kernel_magnetic_force_colloids.cu:15-203, 3D e scaled to |e| = R), over the coarse
+// grid in the reference's order.  One thread per colloid.
+__device__ __forceinline__ int coll_neigh_cells(const BoxParams& p, double x, double y,
+                                                double z, int* cells) {
+  const int* Nc = p.Ncells_colloids;
+  const int cxi = (int)floor(x / p.cell_colloids_size[0]);
+  const int cyi = (int)floor(y / p.cell_colloids_size[1]);
+  const int czi = p.dim == 3 ? (int)floor(z / p.cell_colloids_size[2]) : 0;
+  int n = 0;
+  const int dz0 = p.dim == 3 ? -1 : 0, dz1 = p.dim == 3 ? 1 : 0;
+  for (int dx = -1; dx <= 1; ++dx)
+    for (int dy = -1; dy <= 1; ++dy)
+      for (int dz = dz0; dz <= dz1; ++dz) {
+        int cx = cxi + dx, cy = cyi + dy, cz = czi + dz;
+        if (cx < 0) cx += Nc[0];
+        if (cx >= Nc[0]) cx -= Nc[0];
+        if (p.wall == 0) {
+          if (cy < 0) cy += Nc[1];
+          if (cy >= Nc[1]) cy -= Nc[1];
+        }
+        if (p.dim == 3) {
+          if (cz < 0) cz += Nc[2];
+          if (cz >= Nc[2]) cz -= Nc[2];
+        }
+        if (cy >= 0 && cy < Nc[1])
+          cells[n++] = p.dim == 3 ? cz * Nc[0] * Nc[1] + cy * Nc[0] + cx : cy * Nc[0] + cx;
+      }
+  return n;
+}
+
+__global__ void k_colloid_pairs(Dev d) {
+  const int c = blockIdx.x * blockDim.x + threadIdx.x;
+  if (c >= d.ncoll) return;
+  const int b = d.coll_box[c];
+  const BoxParams& p = d.box[b];
+  if (p.N_colloids < 2) return;
+  const int nc = d.ncoll, c0 = p.coll0, i = c - c0;
+  const double* cs = d.cs;
+  const double xi = cs[CS_X * nc + c], yi = cs[CS_Y * nc + c], zi = cs[CS_Z * nc + c];
+  const double L[3] = {p.L[0], p.L[1], p.L[2]};
+  const double h[3] = {p.halfL[0], p.halfL[1], p.halfL[2]};
+  double F[3] = {cs[CS_FX * nc + c], cs[CS_FY * nc + c], cs[CS_FZ * nc + c]};
+  int cells[27];
+  const int ncell = coll_neigh_cells(p, xi, yi, zi, cells);
+  const double Famp = p.F0_rep * p.tau_rep;
+  const double* m = d.mag + 3 * b;
+  for (int pass = 0; pass < 2; ++pass) {
+    for (int q = 0; q < ncell; ++q) {
+      const int cc = p.ccell0 + cells[q];
+      const int s = d.ccell_start[cc], e = d.ccell_end[cc];
+      for (int k = s; k <= e; ++k) {
+        const int j = d.cindex[c0 + k];
+        if (i == j) continue;
+        double r[3] = {xi - cs[CS_X * nc + c0 + j], yi - cs[CS_Y * nc + c0 + j],
+                       p.dim == 3 ? zi - cs[CS_Z * nc + c0 + j] : 0.0};
+        if (p.dim == 3)
+          min_image<double, 3>(r[0], r[1], r[2], L, h, p.wall);
+        else
+          min_image<double, 2>(r[0], r[1], r[2], L, h, p.wall);
+        double r2 = p.dim == 3 ? r[0] * r[0] + r[1] * r[1] + r[2] * r[2]
+                               : r[0] * r[0] + r[1] * r[1];
+        if (pass == 0) {
+          if (r2 < p.rcuton_coll_rep_sq) r2 = p.rcuton_coll_rep_sq;
+          if (r2 <= p.rcutoff_coll_rep_sq) {
+            const double rr = sqrt(r2);
+            const double ts = -p.tau_rep * (rr - 2.0 * p.coll_R) / p.coll_R;
+            const double ex = exp(ts);
+            const double Fm = Famp * ex / (1.0 - ex);
+            for (int a = 0; a < p.dim; ++a) F[a] = F[a] + Fm * (r[a] / rr);
+          }
+        } else if (r2 <= p.r0_magnet_sq) {
+          const double rr = p.dim == 3 ? sqrt(r2) / p.coll_R : sqrt(r2);
+          const double e[3] = {r[0] / rr, r[1] / rr, p.dim == 3 ? r[2] / rr : 0.0};
+          const double me = p.dim == 3 ? m[0] * e[0] + m[1] * e[1] + m[2] * e[2]
+                                       : m[0] * e[0] + m[1] * e[1];
+          const double me2 = me * me;
+          const double F0r4 = p.F0_magnet / (r2 * r2);
+          for (int a = 0; a < p.dim; ++a)
+            F[a] = F[a] + F0r4 * (2.0 * me * m[a] - (5.0 * me2 - 1.0) * e[a]);
+        }
+      }
+    }
+  }
+  double* csw = d.cs;
+  csw[CS_FX * nc + c] = F[0];
+  csw[CS_FY * nc + c] = F[1];
+  if (p.dim == 3) csw[CS_FZ * nc + c] = F[2];
+}
+
+// Magnetic moment of every box at the context time (main.cu:395-400):
+// m = (cos w t, sin w t, 0), t = t0 + dt * step.  mode 0: next step (step + 1) and count
+// it; mode 1: current step.
+__global__ void k_advance_time(Dev d, int nboxes, int mode) {
+  const int b = blockIdx.x * blockDim.x + threadIdx.x;
+  const long long step = *d.step + (mode == 0 ? 1 : 0);
+  if (b < nboxes) {
+    const BoxParams& p = d.box[b];
+    const double ang = p.omega_magnet * (p.t0 + p.dt * (double)step);
+    d.mag[3 * b + 0] = cos(ang);
+    d.mag[3 * b + 1] = sin(ang);
+    d.mag[3 * b + 2] = 0.0;
+  }
+}
+
+__global__ void k_count_step(Dev d) {
+  if (threadIdx.x == 0 && blockIdx.x == 0) *d.step += 1;
+}
+
+// Kinetic energy per box (kernel_calculate_macro_vars.cu:14-40).  Slots are cut into
+// chunks that never straddle two boxes; each block sums one chunk in a fixed tree order
+// and one thread per box adds its chunks in order, so the sum is reproducible.
+__global__ void __launch_bounds__(kRedThreads) k_ke_partial(Dev d, double* partial) {
+  __shared__ double sh[1][kRedThreads];
+  const int c = blockIdx.x;
+  const int lo = d.ke_chunk[c], hi = d.ke_chunk[c + 1];
+  double v[1] = {0.0};
+  for (int i = lo + threadIdx.x; i < hi; i += kRedThreads) {
+    const double4 x = d.pos[i];
+    const double4 u = d.vel[i];
+    const BoxParams& p = d.box[box_of(d.tinfo[i])];
+    const double v2 = p.dim == 3 ? u.x * u.x + u.y * u.y + u.z * u.z : u.x * u.x + u.y * u.y;
+    v[0] += 0.5 * x.w * v2;
+  }
+  block_reduce<1>(v, sh);
+  if (threadIdx.x == 0) partial[c] = v[0];
+}
+
+__global__ void k_ke_final(Dev d, const double* partial) {
+  const int b = blockIdx.x * blockDim.x + threadIdx.x;
+  if (b >= d.nboxes) return;
+  double ke = 0.0;
+  for (int c = d.ke_box_chunk[b]; c < d.ke_box_chunk[b + 1]; ++c) ke += partial[c];
+  d.ke[b] = ke;
+}
+
+// Field gather / scatter between slot order and original order.
+__device__ __forceinline__ double* field_ptr(const Dev& d, int f, int& comp, bool& in_pos,
+                                             bool& in_vel) {
+  in_pos = in_vel = false;
+  comp = 0;
+  const int Np = d.Npad;
+  switch (f) {
+    case SPH_X: case SPH_Y: case SPH_Z: in_pos = true; comp = f - SPH_X; return nullptr;
+    case SPH_MASS: in_pos = true; comp = 3; return nullptr;
+    case SPH_VX: case SPH_VY: case SPH_VZ: in_vel = true; comp = f - SPH_VX; return nullptr;
+    case SPH_FX: case SPH_FY: case SPH_FZ: return d.f + (f - SPH_FX) * Np;
+    case SPH_DENS: return d.dens;
+    case SPH_PRESS: return d.press;
+    default: break;
+  }
+  if (f >= SPH_CXX && f <= SPH_CZZ) return d.conf + (f - SPH_CXX) * Np;
+  if (f >= SPH_DCDT_XX && f <= SPH_DCDT_ZZ) return d.dcdt + (f - SPH_DCDT_XX) * Np;
+  if (f >= SPH_GXX && f <= SPH_GZZ && d.gradv) return d.gradv + (f - SPH_GXX) * Np;
+  return nullptr;
+}
+
+__global__ void k_gather_field(Dev d, int f, double* out) {
+  const int g = blockIdx.x * blockDim.x + threadIdx.x;
+  if (g >= d.Ntot) return;
+  const int s = d.inv[g];
+  int comp;
+  bool ip, iv;
+  const double* src = field_ptr(d, f, comp, ip, iv);
+  double v = 0.0;
+  if (ip) {
+    const double4 x = d.pos[s];
+    v = comp == 0 ? x.x : comp == 1 ? x.y : comp == 2 ? x.z : x.w;
+  } else if (iv) {
+    const double4 u = d.vel[s];
+    v = comp == 0 ? u.x : comp == 1 ? u.y : u.z;
+  } else if (src) {
+    v = src[s];
+  }
+  out[g] = v;
+}
+
+__global__ void k_scatter_field(Dev d, int f, const double* in) {
+  const int g = blockIdx.x * blockDim.x + threadIdx.x;
+  if (g >= d.Ntot) return;
+  const int s = d.inv[g];
+  int comp;
+  bool ip, iv;
+  double* dst = field_ptr(d, f, comp, ip, iv);
+  const double v = in[g];
+  if (ip) {
+    double4 x = d.pos[s];
+    if (comp == 0) x.x = v; else if (comp == 1) x.y = v; else if (comp == 2) x.z = v; else x.w = v;
+    d.pos[s] = x;
+  } else if (iv) {
+    double4 u = d.vel[s];
+    if (comp == 0) u.x = v; else if (comp == 1) u.y = v; else u.z = v;
+    d.vel[s] = u;
+  } else if (dst) {
+    dst[s] = v;
+  }
+}
+
+__global__ void k_gather_int(Dev d, const int* src, int* out) {
+  const int g = blockIdx.x * blockDim.x + threadIdx.x;
+  if (g >= d.Ntot) return;
+  out[g] = src[d.inv[g]];
+}
+
+// ---------------------------------------------------------------------------------
+// Launchers
+// ---------------------------------------------------------------------------------
+namespace {
+inline cudaStream_t S(const Launch& L) { return static_cast<cudaStream_t>(L.stream); }
+inline int blocks(int n, int t) { return (n + t - 1) / t; }
+inline int check(const Launch& L) {
+  ++*L.launches;
+  const cudaError_t e = cudaGetLastError();
+  if (e == cudaSuccess) return 0;
+  last_launch_error() = (int)e;
+  return 1;
+}
+constexpr int kT = 128;
+}  // namespace
+
+int launch_vv1_particles(const Launch& L) {
+  if (L.d.Ntot == 0) return 0;
+  k_vv1_particles<<<blocks(L.d.Ntot, kT), kT, 0, S(L)>>>(L.d);
+  return check(L);
+}
+
+int launch_vv1_colloids(const Launch& L) {
+  if (L.d.ncoll == 0) return 0;
+  k_vv1_colloids<<<L.d.ncoll, 128, 0, S(L)>>>(L.d);
+  return check(L);
+}
+
+int launch_vv2(const Launch& L) {
+  if (L.d.Ntot > 0) {
+    k_vv2_particles<<<blocks(L.d.Ntot, kT), kT, 0, S(L)>>>(L.d);
+    if (check(L)) return 1;
+  }
+  if (L.d.ncoll > 0) {
+    k_vv2_colloids<<<blocks(L.d.ncoll, kT), kT, 0, S(L)>>>(L.d);
+    if (check(L)) return 1;
+  }
+  return 0;
+}
+
+int launch_hash(const Launch& L) {
+  k_hash<<<blocks(L.d.Ntot, kT), kT, 0, S(L)>>>(L.d);
+  return check(L);
+}
+
+int launch_reorder(const Launch& L, bool permute_forces) {
+  const int nb = blocks(L.d.Ntot, kT);
+  const bool mixed = L.d.pos_f != nullptr;
+  if (mixed && permute_forces) k_reorder<true, true><<<nb, kT, 0, S(L)>>>(L.d);
+  else if (mixed) k_reorder<true, false><<<nb, kT, 0, S(L)>>>(L.d);
+  else if (permute_forces) k_reorder<false, true><<<nb, kT, 0, S(L)>>>(L.d);
+  else k_reorder<false, false><<<nb, kT, 0, S(L)>>>(L.d);
+  return check(L);
+}
+
+int launch_build_lists_dim(const Launch& L, int dim) {
+  if (L.d.Ctot == 0) return 0;
+  const int nb = blocks(L.d.Ctot, kListWarps);
+  if (dim == 3)
+    k_build_lists<3><<<nb, kListWarps * 32, 0, S(L)>>>(L.d);
+  else
+    k_build_lists<2><<<nb, kListWarps * 32, 0, S(L)>>>(L.d);
+  return check(L);
+}
+
+int launch_colloid_cells_n(const Launch& L, int nboxes, int max_coll) {
+  if (L.d.ncoll == 0) return 0;
+  k_colloid_cells<<<nboxes, 128, sizeof(int) * (max_coll > 0 ? max_coll : 1), S(L)>>>(L.d, nboxes);
+  return check(L);
+}
+
+int launch_density_dim(const Launch& L, int dim) {
+  const int nb = blocks(L.d.Ntot, kT);
+  if (L.prec == SPH_PREC_FP64) {
+    if (dim == 3) k_density<double, 3><<<nb, kT, 0, S(L)>>>(L.d);
+    else k_density<double, 2><<<nb, kT, 0, S(L)>>>(L.d);
+  } else {
+    if (dim == 3) k_density<float, 3><<<nb, kT, 0, S(L)>>>(L.d);
+    else k_density<float, 2><<<nb, kT, 0, S(L)>>>(L.d);
+  }
+  return check(L);
+}
+
+int launch_pressure(const Launch& L) {
+  const int nb = blocks(L.d.Ntot, kT);
+  if (L.prec == SPH_PREC_FP64)
+    k_pressure<double><<<nb, kT, 0, S(L)>>>(L.d);
+  else
+    k_pressure<float><<<nb, kT, 0, S(L)>>>(L.d);
+  return check(L);
+}
+
+template <typename T, int DIM>
+static void pairs_dispatch(const Launch& L, int mode, int with_ext, int nb) {
+  if (mode == kPairGradvAll)
+    k_pairs<T, DIM, kPairGradvAll, false><<<nb, 128, 0, S(L)>>>(L.d);
+  else if (mode == kPairForcesOnly)
+    k_pairs<T, DIM, kPairForcesOnly, false><<<nb, 128, 0, S(L)>>>(L.d);
+  else if (with_ext)
+    k_pairs<T, DIM, kPairFused, true><<<nb, 128, 0, S(L)>>>(L.d);
+  else
+    k_pairs<T, DIM, kPairFused, false><<<nb, 128, 0, S(L)>>>(L.d);
+}
+
+int launch_pairs_dim(const Launch& L, int dim, int mode, int with_ext) {
+  const int nb = blocks(L.d.Ntot, 128);
+  if (L.prec == SPH_PREC_FP64) {
+    if (dim == 3) pairs_dispatch<double, 3>(L, mode, with_ext, nb);
+    else pairs_dispatch<double, 2>(L, mode, with_ext, nb);
+  } else {
+    if (dim == 3) pairs_dispatch<float, 3>(L, mode, with_ext, nb);
+    else pairs_dispatch<float, 2>(L, mode, with_ext, nb);
+  }
+  return check(L);
+}
+
+int launch_ext_force(const Launch& L) {
+  k_ext_force<<<blocks(L.d.Ntot, kT), kT, 0, S(L)>>>(L.d);
+  return check(L);
+}
+
+int launch_dcdt_from_gradv(const Launch& L) {
+  k_dcdt<<<blocks(L.d.Ntot, kT), kT, 0, S(L)>>>(L.d);
+  return check(L);
+}
+
+int launch_wall_forces(const Launch& L) {
+  if (L.d.nwallseg == 0) return 0;
+  k_wall_forces<<<L.d.nwallseg, kRedThreads, 0, S(L)>>>(L.d);
+  return check(L);
+}
+
+int launch_colloid_forces(const Launch& L, int with_pairs) {
+  if (L.d.ncoll == 0) return 0;
+  k_collect_colloids<<<L.d.ncoll, kRedThreads, 0, S(L)>>>(L.d);
+  if (check(L)) return 1;
+  if (with_pairs) {
+    k_colloid_pairs<<<blocks(L.d.ncoll, 64), 64, 0, S(L)>>>(L.d);
+    if (check(L)) return 1;
+  }
+  return 0;
+}
+
+int launch_advance_time(const Launch& L, int mode) {
+  k_advance_time<<<blocks(L.d.nboxes, 64), 64, 0, S(L)>>>(L.d, L.d.nboxes, mode);
+  return check(L);
+}
+
+int launch_count_step(const Launch& L) {
+  k_count_step<<<1, 32, 0, S(L)>>>(L.d);
+  return check(L);
+}
+
+int launch_kinetic_energy(const Launch& L, double* partial) {
+  k_ke_partial<<<L.d.nkechunks, kRedThreads, 0, S(L)>>>(L.d, partial);
+  if (check(L)) return 1;
+  k_ke_final<<<blocks(L.d.nboxes, 64), 64, 0, S(L)>>>(L.d, partial);
+  return check(L);
+}
+
+int launch_gather_field(const Launch& L, int field, double* out) {
+  k_gather_field<<<blocks(L.d.Ntot, kT), kT, 0, S(L)>>>(L.d, field, out);
+  return check(L);
+}
+
+int launch_scatter_field(const Launch& L, int field, const double* in) {
+  k_scatter_field<<<blocks(L.d.Ntot, kT), kT, 0, S(L)>>>(L.d, field, in);
+  return check(L);
+}
+
+int launch_gather_int(const Launch& L, const int* src, int* out) {
+  k_gather_int<<<blocks(L.d.Ntot, kT), kT, 0, S(L)>>>(L.d, src, out);
+  return check(L);
+}
+
+}  // namespace sph

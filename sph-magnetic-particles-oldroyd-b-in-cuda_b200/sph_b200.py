@@ -1,0 +1,324 @@
+"""Python host API of the B200 SPH engine (ctypes over lib/libsph_b200.so).
+
+The class `System` mirrors the reference's `class_system` step methods
+(src/class_system.h:344-650): neighbours_search, calculate_density, calculate_pressure,
+calculate_vel_gradient, calculate_forces, calculate_external_forces,
+calculate_force_walls, calculate_force_colloids, V_Verlet_step1, V_Verlet_step2; plus
+`step(n)`, the driver loop of src/main.cu:358-467 replayed as a CUDA graph.  Arrays come
+back in the reference's original particle order.
+
+There is no CPU fallback: importing works anywhere, but creating a System needs the
+compiled library and a CUDA device, and raises otherwise.
+"""
+import ctypes
+import os
+import subprocess
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(HERE, "lib", "libsph_b200.so")
+
+FIELDS = [
+    "x", "y", "z", "vx", "vy", "vz", "fx", "fy", "fz", "dens", "press", "mass",
+    "cxx", "cxy", "cyy", "cxz", "cyz", "czz", "dcdt_xx", "dcdt_xy", "dcdt_yy",
+    "dcdt_xz", "dcdt_yz", "dcdt_zz", "gxx", "gxy", "gxz", "gyx", "gyy", "gyz", "gzx",
+    "gzy", "gzz",
+]
+COLLOID_FIELDS = [
+    "coll_x", "coll_y", "coll_z", "coll_vx", "coll_vy", "coll_vz", "coll_omegax",
+    "coll_omegay", "coll_omegaz", "coll_theta", "coll_quat0", "coll_quatx", "coll_quaty",
+    "coll_quatz", "fx_colloid", "fy_colloid", "fz_colloid", "tx_colloid", "ty_colloid",
+    "tz_colloid",
+]
+STATUS = {
+    0: "SPH_OK", 1: "SPH_ERR_BAD_INPUT", 2: "SPH_ERR_CUDA", 3: "SPH_ERR_CELL_RANGE",
+    4: "SPH_ERR_NAN", 5: "SPH_ERR_TIMEOUT", 6: "SPH_ERR_STATE", 7: "SPH_ERR_NOMEM",
+    8: "SPH_ERR_CAPACITY", 9: "SPH_ERR_IO",
+}
+PRECISION = {"fp64": 0, "mixed": 1}
+
+# every symbol include/sph_capi.h declares
+EXPORTS = [
+    "sph_read_input", "sph_create", "sph_create_ensemble", "sph_destroy", "sph_get_info",
+    "sph_last_error", "sph_status_string", "sph_neighbours_search", "sph_calculate_density",
+    "sph_calculate_pressure", "sph_calculate_vel_gradient", "sph_calculate_forces",
+    "sph_calculate_external_forces", "sph_calculate_force_walls",
+    "sph_calculate_force_colloids", "sph_vv_step1", "sph_vv_step2", "sph_initial_forces",
+    "sph_step", "sph_synchronize", "sph_read_field", "sph_write_field",
+    "sph_read_field_device", "sph_read_type", "sph_read_colloid_field",
+    "sph_read_wall_forces", "sph_export_cells", "sph_export_colloid_cells",
+    "sph_kinetic_energy", "sph_last_step_ms", "sph_kernel_launches",
+]
+
+c_int, c_double, c_void_p, c_char_p = ctypes.c_int, ctypes.c_double, ctypes.c_void_p, ctypes.c_char_p
+PD = ctypes.POINTER(ctypes.c_double)
+PI = ctypes.POINTER(ctypes.c_int)
+
+
+class SphInput(ctypes.Structure):
+    _fields_ = [
+        ("N", c_int * 3), ("L", c_double * 3), ("dim", c_int), ("dt", c_double),
+        ("t0", c_double), ("Nsteps", c_int), ("overlap", c_double), ("rho", c_double),
+        ("c", c_double), ("P0", c_double), ("eta", c_double), ("zeta", c_double),
+        ("np", c_double), ("kT", c_double), ("tau", c_double), ("ext_force_type", c_int),
+        ("ext_force", c_double * 3), ("freq_micro", c_int), ("freq_macro", c_int),
+        ("freq_walls", c_int), ("freq_colloids", c_int), ("wall", c_int),
+        ("Vwall_top", c_double), ("Vwall_bottom", c_double), ("N_colloids", c_int),
+        ("coll_R", c_double), ("coll_rho", c_double), ("coll_xyz", PD), ("coll_move", c_int),
+        ("coll_repulsion_cuton", c_double), ("F0_repulsion", c_double),
+        ("tau_repulsion", c_double), ("cutoff_magnetic", c_double), ("F0_magnetic", c_double),
+        ("omega_magnetic", c_double), ("new_sim", c_int),
+    ]
+
+
+class SphOptions(ctypes.Structure):
+    _fields_ = [("precision", c_int), ("device", c_int), ("use_graph", c_int),
+                ("nbr_capacity", c_int)]
+
+
+class SphInfo(ctypes.Structure):
+    _fields_ = [
+        ("N", c_int), ("dim", c_int), ("wall", c_int), ("Ncells", c_int * 3),
+        ("Ntotal_cells", c_int), ("Nwalls", c_int), ("Nlist_walls", c_int),
+        ("N_colloids", c_int), ("Nlist_colloids", c_int), ("Ncells_colloids", c_int * 3),
+        ("Ntotal_cells_colloids", c_int), ("step", c_int), ("nboxes", c_int),
+        ("precision", c_int),
+        ("rcut", c_double), ("rcutsq", c_double), ("cw", c_double), ("c_gradw", c_double),
+        ("csq", c_double), ("rho0", c_double), ("a", c_double), ("b", c_double),
+        ("nkT", c_double), ("tau", c_double), ("dt", c_double), ("cell_size", c_double * 3),
+        ("wall_width", c_double), ("y_bottom", c_double), ("y_top", c_double),
+        ("V_bottom", c_double), ("V_top", c_double), ("coll_R", c_double),
+        ("coll_mass", c_double), ("coll_I", c_double), ("L", c_double * 3), ("t0", c_double),
+        ("omega_magnet", c_double),
+    ]
+
+
+_lib = None
+
+
+class SphError(RuntimeError):
+    def __init__(self, status, msg):
+        self.status = STATUS.get(status, str(status))
+        super().__init__("%s: %s" % (self.status, msg))
+
+
+def build():
+    subprocess.run(["make", "-s", "-C", HERE], check=True)
+
+
+def lib():
+    """Load the engine library; raises if it has not been built."""
+    global _lib
+    if _lib is None:
+        if not os.path.exists(LIB_PATH):
+            raise RuntimeError("engine library missing: %s (run make in %s)" % (LIB_PATH, HERE))
+        L = ctypes.CDLL(LIB_PATH)
+        L.sph_read_input.argtypes = [c_char_p, ctypes.POINTER(SphInput), PD, c_int, c_char_p, ctypes.c_size_t]
+        L.sph_create.argtypes = [ctypes.POINTER(SphInput), c_char_p, ctypes.POINTER(SphOptions), ctypes.POINTER(c_void_p)]
+        L.sph_create_ensemble.argtypes = [c_int, ctypes.POINTER(SphInput), ctypes.POINTER(c_char_p),
+                                          ctypes.POINTER(SphOptions), ctypes.POINTER(c_void_p)]
+        L.sph_destroy.argtypes = [c_void_p]
+        L.sph_destroy.restype = None
+        L.sph_get_info.argtypes = [c_void_p, c_int, ctypes.POINTER(SphInfo)]
+        L.sph_last_error.argtypes = [c_void_p]
+        L.sph_last_error.restype = c_char_p
+        L.sph_status_string.argtypes = [c_int]
+        L.sph_status_string.restype = c_char_p
+        for n in ["sph_neighbours_search", "sph_calculate_density", "sph_calculate_pressure",
+                  "sph_calculate_vel_gradient", "sph_calculate_external_forces",
+                  "sph_calculate_force_walls", "sph_vv_step1", "sph_vv_step2",
+                  "sph_initial_forces", "sph_synchronize"]:
+            getattr(L, n).argtypes = [c_void_p]
+        L.sph_calculate_forces.argtypes = [c_void_p, PD]
+        L.sph_calculate_force_colloids.argtypes = [c_void_p, PD]
+        L.sph_step.argtypes = [c_void_p, c_int]
+        L.sph_read_field.argtypes = [c_void_p, c_int, PD]
+        L.sph_write_field.argtypes = [c_void_p, c_int, PD]
+        L.sph_read_field_device.argtypes = [c_void_p, c_int, c_void_p]
+        L.sph_read_type.argtypes = [c_void_p, PI]
+        L.sph_read_colloid_field.argtypes = [c_void_p, c_int, PD]
+        L.sph_read_wall_forces.argtypes = [c_void_p, PD]
+        L.sph_export_cells.argtypes = [c_void_p, PI, PI, PI, PI]
+        L.sph_export_colloid_cells.argtypes = [c_void_p, PI, PI, PI, PI]
+        L.sph_kinetic_energy.argtypes = [c_void_p, PD]
+        L.sph_last_step_ms.argtypes = [c_void_p, PD]
+        L.sph_kernel_launches.argtypes = [c_void_p, ctypes.POINTER(ctypes.c_longlong)]
+        _lib = L
+    return _lib
+
+
+def read_input(path):
+    """Parse a reference `input` file with the engine's parser; returns (SphInput, coll)."""
+    inp = SphInput()
+    coll = np.zeros(3 * 1000, dtype=np.float64)
+    msg = ctypes.create_string_buffer(256)
+    st = lib().sph_read_input(path.encode(), ctypes.byref(inp), coll.ctypes.data_as(PD), 1000, msg, 256)
+    if st != 0:
+        raise SphError(st, msg.value.decode())
+    return inp, coll
+
+
+class System:
+    """One or more simulation boxes on the GPU (the reference's class_system)."""
+
+    def __init__(self, input_paths, particles_paths=None, precision="fp64", use_graph=True,
+                 device=0, nbr_capacity=0):
+        if isinstance(input_paths, (str, os.PathLike)):
+            input_paths = [input_paths]
+        n = len(input_paths)
+        self._keep = []
+        arr = (SphInput * n)()
+        for b, path in enumerate(input_paths):
+            inp, coll = read_input(str(path))
+            self._keep.append(coll)
+            arr[b] = inp
+            arr[b].coll_xyz = coll.ctypes.data_as(PD)
+        paths = (c_char_p * n)()
+        for b in range(n):
+            p = particles_paths[b] if particles_paths else None
+            paths[b] = p.encode() if p else None
+        opt = SphOptions(PRECISION[precision], device, 1 if use_graph else 0, nbr_capacity)
+        h = c_void_p()
+        st = lib().sph_create_ensemble(n, arr, paths, ctypes.byref(opt), ctypes.byref(h))
+        if st != 0:
+            raise SphError(st, "sph_create failed (see stderr)")
+        self._h = h
+        self.nboxes = n
+        self.precision = precision
+        self._info = [self.info(b) for b in range(n)]
+        self.N = sum(i["N"] for i in self._info)
+        self.ncoll = sum(i["N_colloids"] for i in self._info)
+
+    def close(self):
+        if getattr(self, "_h", None):
+            lib().sph_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def _ok(self, st):
+        if st != 0:
+            raise SphError(st, lib().sph_last_error(self._h).decode())
+
+    def info(self, box=0):
+        o = SphInfo()
+        self._ok(lib().sph_get_info(self._h, box, ctypes.byref(o)))
+        out = {}
+        for name, _ in SphInfo._fields_:
+            v = getattr(o, name)
+            out[name] = list(v) if isinstance(v, ctypes.Array) else v
+        return out
+
+    # --- class_system methods ---
+    def neighbours_search(self):
+        self._ok(lib().sph_neighbours_search(self._h))
+
+    def calculate_density(self):
+        self._ok(lib().sph_calculate_density(self._h))
+
+    def calculate_pressure(self):
+        self._ok(lib().sph_calculate_pressure(self._h))
+
+    def calculate_vel_gradient(self):
+        self._ok(lib().sph_calculate_vel_gradient(self._h))
+
+    @staticmethod
+    def _m(m):
+        if m is None:
+            return None
+        a = np.ascontiguousarray(m, dtype=np.float64)
+        return a
+
+    def calculate_forces(self, m=None):
+        a = self._m(m)
+        self._ok(lib().sph_calculate_forces(self._h, a.ctypes.data_as(PD) if a is not None else None))
+
+    def calculate_external_forces(self):
+        self._ok(lib().sph_calculate_external_forces(self._h))
+
+    def calculate_force_walls(self):
+        self._ok(lib().sph_calculate_force_walls(self._h))
+
+    def calculate_force_colloids(self, m=None):
+        a = self._m(m)
+        self._ok(lib().sph_calculate_force_colloids(self._h, a.ctypes.data_as(PD) if a is not None else None))
+
+    def V_Verlet_step1(self):
+        self._ok(lib().sph_vv_step1(self._h))
+
+    def V_Verlet_step2(self):
+        self._ok(lib().sph_vv_step2(self._h))
+
+    def initial_forces(self):
+        self._ok(lib().sph_initial_forces(self._h))
+
+    def step(self, n=1):
+        self._ok(lib().sph_step(self._h, int(n)))
+
+    def synchronize(self):
+        self._ok(lib().sph_synchronize(self._h))
+
+    def last_step_ms(self):
+        v = c_double()
+        self._ok(lib().sph_last_step_ms(self._h, ctypes.byref(v)))
+        return v.value
+
+    def kernel_launches(self):
+        v = ctypes.c_longlong()
+        self._ok(lib().sph_kernel_launches(self._h, ctypes.byref(v)))
+        return v.value
+
+    # --- state ---
+    def field(self, name):
+        out = np.empty(self.N, dtype=np.float64)
+        self._ok(lib().sph_read_field(self._h, FIELDS.index(name), out.ctypes.data_as(PD)))
+        return out
+
+    def set_field(self, name, values):
+        a = np.ascontiguousarray(values, dtype=np.float64)
+        assert a.shape == (self.N,)
+        self._ok(lib().sph_write_field(self._h, FIELDS.index(name), a.ctypes.data_as(PD)))
+
+    def type(self):
+        out = np.empty(self.N, dtype=np.int32)
+        self._ok(lib().sph_read_type(self._h, out.ctypes.data_as(PI)))
+        return out
+
+    def colloid_field(self, name):
+        out = np.zeros(max(self.ncoll, 0), dtype=np.float64)
+        if self.ncoll:
+            self._ok(lib().sph_read_colloid_field(self._h, COLLOID_FIELDS.index(name), out.ctypes.data_as(PD)))
+        return out
+
+    def wall_forces(self):
+        """(nboxes, 2 walls, 3) wall forces."""
+        out = np.zeros(6 * self.nboxes, dtype=np.float64)
+        self._ok(lib().sph_read_wall_forces(self._h, out.ctypes.data_as(PD)))
+        return out.reshape(self.nboxes, 2, 3)
+
+    def export_cells(self):
+        i0 = self._info[0]
+        pc = np.empty(i0["N"], dtype=np.int32)
+        pi = np.empty(i0["N"], dtype=np.int32)
+        cs = np.empty(i0["Ntotal_cells"], dtype=np.int32)
+        ce = np.empty(i0["Ntotal_cells"], dtype=np.int32)
+        self._ok(lib().sph_export_cells(self._h, pc.ctypes.data_as(PI), pi.ctypes.data_as(PI),
+                                        cs.ctypes.data_as(PI), ce.ctypes.data_as(PI)))
+        return dict(particle_cell=pc, particle_index=pi, cell_start=cs, cell_end=ce)
+
+    def export_colloid_cells(self):
+        i0 = self._info[0]
+        n, m = i0["N_colloids"], i0["Ntotal_cells_colloids"]
+        a = [np.zeros(n, np.int32), np.zeros(n, np.int32), np.zeros(m, np.int32), np.zeros(m, np.int32)]
+        self._ok(lib().sph_export_colloid_cells(self._h, *[x.ctypes.data_as(PI) for x in a]))
+        return dict(coll_cell=a[0], coll_index=a[1], coll_cell_start=a[2], coll_cell_end=a[3])
+
+    def kinetic_energy(self):
+        out = np.zeros(self.nboxes, dtype=np.float64)
+        self._ok(lib().sph_kinetic_energy(self._h, out.ctypes.data_as(PD)))
+        return out
