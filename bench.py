@@ -1,0 +1,333 @@
+#!/usr/bin/env python
+"""Benchmark: particle-steps/s of the SPH step on the 128^3 Oldroyd-B Couette workload.
+
+Workload (the reference's headline configuration, 3D Couette flow): 128^3 lattice between
+y-walls (128 x 134 x 128 = 2,195,456 particles including the wall layers), L = 1,
+overlap = 3, V_wall = -0.5 / +0.5, rho = 1, c = 10, P0 = 0, eta = 0.1, zeta = 0,
+np = 100, kT = 0.01, tau = 1, dt = 2e-5; synthetic initial state (lattice, fluid at rest,
+c = I).  A step is the reference driver's step (main.cu:358-467): half-kick and drift,
+neighbour search, density, velocity gradient, forces, dc/dt, wall forces, half-kick.
+
+  python bench.py [--gpus N] [--steps K] [--warmup W] [--precision fp64|mixed]
+  python bench.py --impl reference ...    # the reference's own CUDA build, same workload
+
+value : K * N_particles * n_ranks / (max over ranks of the device time of K steps),
+        measured with CUDA events on the engine's stream around one sph_step(K) call
+        (CUDA-graph replay), inputs resident in HBM.  The state (~0.7 GB) is larger than
+        the 126 MB L2, so no L2 flush is needed between steps.
+e2e   : the same metric through the reference-facing C ABI with host buffers: every step
+        calls V_Verlet_step1, neighbours_search, calculate_forces(m) with the magnetic
+        moment copied from host memory, V_Verlet_step2, then reads the wall forces and the
+        kinetic energy back to the host (wall-clock time).
+With N > 1 GPUs every rank advances its own replica of the box (the single box does not
+shard; replicas only): weak scaling, no collective in the data path.
+"""
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import tempfile
+import time
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+PKG = os.path.join(ROOT, "sph-magnetic-particles-oldroyd-b-in-cuda_b200")
+for p in (PKG, os.path.join(ROOT, "oracle")):
+    if p not in sys.path:
+        sys.path.insert(0, p)
+
+import numpy as np  # noqa: E402
+
+import sph_input  # noqa: E402
+
+WORKLOAD = dict(N=(128, 128, 128), L=(1.0, 1.0, 1.0), dim=3, overlap=3.0, wall=1,
+                Vwall_bottom=-0.5, Vwall_top=0.5, rho=1.0, c=10.0, P0=0.0, eta=0.1, zeta=0.0,
+                np=100.0, kT=0.01, tau=1.0, dt=2e-5)
+WORKLOAD_NAME = "couette3d_128: 128^3 Oldroyd-B Couette flow between y-walls, 2,195,456 particles"
+METRIC = "particle-steps/s (128^3 Oldroyd-B Couette)"
+UNIT = "particle-steps/s"
+# Algorithmic bytes per particle-step of the whole step (four grid-wide phases, each
+# per-particle field read once and written once): (10 d + 5 n_c + 4) P + 28 with d = 3,
+# n_c = 6 conformation components, P = bytes per real.
+B_ALG_STEP = {"fp64": (10 * 3 + 5 * 6 + 4) * 8 + 28, "mixed": 380}
+# Algorithmic bytes per particle of one launch of the fused pair kernel (k_pairs):
+# reads x, v (6 reals), Pi/d^2 (6), 1/d, p, c (6), mass (1) and the type word; writes
+# f (3) and dc/dt (6).
+B_ALG_PAIRS = {"fp64": (6 + 6 + 1 + 1 + 6 + 1 + 3 + 6) * 8 + 4,
+               "mixed": (6 + 6 + 1) * 4 + (1 + 6 + 1 + 3 + 6) * 8 + 4}
+
+
+def peaks():
+    path = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    if os.path.exists(path):
+        with open(path) as f:
+            d = json.load(f)
+        return float(d["hbm_gbs"]), "measured"
+    return 6650.0, "fallback"
+
+
+class ClockSampler:
+    """nvidia-smi clocks and throttle reasons sampled every 200 ms while running."""
+
+    Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+         "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+         "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, device):
+        self.device = device
+        self.proc = None
+        self.path = tempfile.mktemp(suffix=".csv")
+
+    def __enter__(self):
+        try:
+            self.f = open(self.path, "w")
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", "-i", str(self.device), "--query-gpu=" + self.Q,
+                 "--format=csv,noheader,nounits", "-lms", "200"], stdout=self.f,
+                stderr=subprocess.DEVNULL)
+        except OSError:
+            self.proc = None
+        time.sleep(0.3)
+        return self
+
+    def __exit__(self, *a):
+        if self.proc:
+            time.sleep(0.25)
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except subprocess.TimeoutExpired:
+                self.proc.kill()
+            self.f.close()
+
+    def summary(self):
+        if not self.proc:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        sm, smax, reasons = [], [], set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        with open(self.path) as f:
+            for line in f:
+                p = [t.strip() for t in line.split(",")]
+                if len(p) < 9:
+                    continue
+                try:
+                    sm.append(float(p[1]))
+                    smax.append(float(p[2]))
+                except ValueError:
+                    continue
+                for k, name in enumerate(names):
+                    if p[5 + k].lower() == "active":
+                        reasons.add(name)
+        if not sm:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["no samples"]}
+        return {"sm_mhz": statistics.median(sm), "sm_max_mhz": max(smax),
+                "samples": len(sm), "reasons": sorted(reasons)}
+
+
+def write_workload(d, lattice=128):
+    """The Couette input; lattice < 128 gives a smaller box of the same physics, used only
+    for ncu captures that must stay small."""
+    path = os.path.join(d, "input")
+    spec = dict(WORKLOAD)
+    spec["N"] = (lattice, lattice, lattice)
+    sph_input.write_input(path, **spec)
+    return path
+
+
+def cpu_baseline(workdir, steps=1):
+    """The FP64 OpenMP oracle on this host: initial forces, then `steps` timed steps."""
+    import oracle
+
+    cores = oracle.set_threads(os.cpu_count() or 1)
+    o = oracle.Oracle(write_workload(workdir))
+    o.run(0)
+    t0 = time.perf_counter()
+    o.run(steps)
+    dt = time.perf_counter() - t0
+    n = o.info()["N"]
+    o.close()
+    return {"value": n * steps / dt, "unit": UNIT, "cores": cores, "kind": "port",
+            "sample": "CPU oracle (C99+OpenMP FP64 restatement) on the full 128^3 workload: "
+                      "initial forces untimed, then %d timed step(s), %.1f s" % (steps, dt)}
+
+
+def dist_setup(args):
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    if world > 1:
+        import datetime
+
+        import torch
+        import torch.distributed as dist
+
+        torch.cuda.set_device(local)
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300))
+        return world, rank, local, dist
+    return 1, 0, local, None
+
+
+def max_over_ranks(dist, value, local):
+    if dist is None:
+        return value
+    import torch
+
+    t = torch.tensor([value], dtype=torch.float64, device="cuda:%d" % local)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+def run_reference(args, world, rank, dist):
+    """The reference's own CUDA build (oracle/_ref/ref_sph: its unmodified sources driven by
+    oracle/ref_harness.cu), timed with CUDA events around the step loop."""
+    if rank != 0:
+        return 0
+    ref = os.path.join(ROOT, "oracle", "_ref", "ref_sph")
+    line = {"impl": "reference", "metric": METRIC, "unit": UNIT, "n_gpus": 1, "steps": args.steps,
+            "warmup": args.warmup, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+            "dtype": "f64", "data": "synthetic",
+            "config": {"workload": WORKLOAD_NAME, "implementation": "reference CUDA build, FP64, "
+                                                                  "sm_100a, as shipped"}}
+    if not os.path.exists(ref):
+        line["unavailable"] = "reference build oracle/_ref/ref_sph is missing (build() compiles it)"
+        print(json.dumps(line))
+        return 0
+    with tempfile.TemporaryDirectory() as wd:
+        write_workload(wd)
+        with ClockSampler(int(os.environ.get("LOCAL_RANK", "0"))) as clk:
+            r = subprocess.run([ref, "time", str(args.steps), str(args.warmup)], cwd=wd,
+                               capture_output=True, text=True, timeout=3600)
+        if r.returncode != 0:
+            line["unavailable"] = "reference build failed: rc %d %s" % (r.returncode, r.stderr[-200:])
+            print(json.dumps(line))
+            return 0
+        res = json.loads(r.stdout.strip().splitlines()[-1])
+    sec = res["event_s"]
+    value = res["N"] * args.steps / sec
+    line.update(value=value, ms_per_step=1e3 * sec / args.steps,
+                cpu_baseline={"value": value, "unit": UNIT, "cores": None, "kind": "reference",
+                              "device": "cuda",
+                              "sample": "the reference's own CUDA implementation of the step "
+                                        "(it has no CPU path) on this GPU: %d timed steps after %d "
+                                        "warm-up steps, CUDA events around the loop"
+                                        % (args.steps, args.warmup)},
+                e2e={"value": res["N"] * args.steps / res["wall_s"], "unit": UNIT,
+                     "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+                clocks=clk.summary(), gpu_launches=None)
+    line["config"]["particles"] = res["N"]
+    print(json.dumps(line))
+    return 0
+
+
+def run_ours(args, world, rank, local, dist):
+    import sph_b200
+
+    with tempfile.TemporaryDirectory() as wd:
+        path = write_workload(wd, args.lattice)
+        sysm = sph_b200.System(path, precision=args.precision, device=local)
+        n = sysm.N
+        sysm.step(args.warmup)
+        sysm.synchronize()
+        if dist is not None:
+            dist.barrier()
+        l0 = sysm.kernel_launches()
+        with ClockSampler(local) as clk:
+            sysm.step(args.steps)
+            sysm.synchronize()
+        ms = sysm.last_step_ms()
+        launches = sysm.kernel_launches() - l0
+        if dist is not None:
+            dist.barrier()
+        ms_max = max_over_ranks(dist, ms, local)
+        value = n * args.steps * world / (ms_max * 1e-3)
+        # per-phase device times (CUDA events on the engine's stream), separate short pass
+        phases = sysm.profile_phases(args.profile_steps)
+        # e2e: the reference's call sequence through the C ABI with host buffers
+        ke = []
+        m = np.zeros(3)
+        e2e_steps = min(args.steps, args.e2e_steps)
+        info = sysm.info()
+        t0 = time.perf_counter()
+        for k in range(e2e_steps):
+            step = info["step"] + k + 1
+            ang = info["omega_magnet"] * (info["t0"] + info["dt"] * step)
+            m[0], m[1] = np.cos(ang), np.sin(ang)
+            sysm.V_Verlet_step1()
+            sysm.neighbours_search()
+            sysm.calculate_forces(m)
+            sysm.V_Verlet_step2()
+            wf = sysm.wall_forces()
+            ke.append(float(sysm.kinetic_energy()[0]) + 0.0 * float(wf[0, 0, 0]))
+        e2e_dt = time.perf_counter() - t0
+        e2e_dt = max_over_ranks(dist, e2e_dt, local)
+        sysm.close()
+    if rank != 0:
+        return 0
+    hbm, peak_kind = peaks()
+    pair_ms = phases["pairs"]
+    achieved = B_ALG_PAIRS[args.precision] * n / (pair_ms * 1e-3) / 1e9
+    step_gbs = B_ALG_STEP[args.precision] * n * args.steps / (ms * 1e-3) / 1e9
+    line = {
+        "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": ms_max / args.steps, "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None,
+        "dtype": "f64" if args.precision == "fp64" else "f32 pairs / f64 state",
+        "data": "synthetic (lattice initial state)",
+        "config": {"workload": WORKLOAD_NAME, "particles": n, "precision": args.precision,
+                   "parallelism": "replicas only" if world > 1 else "single box",
+                   "l2": "inputs larger than L2 (state ~0.7 GB > 126 MB), no flush",
+                   "timing": "CUDA events around sph_step(K) on the engine stream, max over ranks"},
+        "roofline": {"kernel": "k_pairs (fused velocity gradient, forces, dc/dt)",
+                     "bound": "hbm", "achieved": achieved, "peak": hbm, "unit": "GB/s",
+                     "frac": achieved / hbm, "peak_kind": peak_kind,
+                     "traffic": args.pairs_traffic,
+                     "note": "pair kernel is FP64/FP32-pipe bound (see profiles/); the HBM "
+                             "fraction is reported as the metric asks"},
+        "hbm_frac_step": step_gbs / hbm,
+        "phase_ms": phases,
+        "e2e": {"value": n * e2e_steps / e2e_dt, "unit": UNIT, "h2d_bytes_per_step": 24,
+                "d2h_bytes_per_step": 2 * 3 * 8 + 8, "steps": e2e_steps},
+        "gpu_launches": launches,
+        "clocks": clk.summary(),
+    }
+    if world == 1 and not args.no_cpu_baseline:
+        with tempfile.TemporaryDirectory() as wd:
+            line["cpu_baseline"] = cpu_baseline(wd, steps=1)
+    print(json.dumps(line))
+    return 0
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=50)
+    ap.add_argument("--warmup", type=int, default=5)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--precision", default="fp64", choices=["fp64", "mixed"])
+    ap.add_argument("--profile-steps", type=int, default=5)
+    ap.add_argument("--e2e-steps", type=int, default=20)
+    ap.add_argument("--pairs-traffic", type=float, default=None,
+                    help="ncu dram bytes per k_pairs launch, if measured")
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--lattice", type=int, default=128,
+                    help="lattice side; 128 is the benchmark, smaller sizes only for ncu captures")
+    args = ap.parse_args()
+    if args.lattice != 128:
+        global WORKLOAD_NAME
+        WORKLOAD_NAME = "couette3d_%d (profiling size, not the benchmark)" % args.lattice
+        args.no_cpu_baseline = True
+    if args.warmup < 3:
+        args.warmup = 3
+    world, rank, local, dist = dist_setup(args)
+    try:
+        if args.impl == "reference":
+            return run_reference(args, world, rank, dist)
+        return run_ours(args, world, rank, local, dist)
+    finally:
+        if dist is not None:
+            dist.destroy_process_group()
+
+
+if __name__ == "__main__":
+    sys.exit(main())

@@ -240,6 +240,15 @@ sph_status sph_last_step_ms(sph_ctx* ctx, double* ms);
 /* Launch counters: kernels launched by the engine since creation. */
 sph_status sph_kernel_launches(const sph_ctx* ctx, long long* count);
 
+/* Profiling (no reference counterpart; the reference times with clock(), main.cu:381-427):
+   runs nsteps full steps with CUDA events between the phases on the context's stream and
+   writes the mean device time of each phase in milliseconds to ms[0..SPH_NUM_PHASES-1]. */
+#define SPH_NUM_PHASES 11
+sph_status sph_profile_phases(sph_ctx* ctx, int nsteps, double* ms);
+/* Name of phase k ("vv1", "hash", "sort", "reorder", "lists", "colloid_cells",
+   "density", "pairs", "walls", "colloids", "vv2"). */
+const char* sph_phase_name(int k);
+
 #ifdef __cplusplus
 }
 #endif

@@ -795,6 +795,77 @@ sph_status sph_kernel_launches(const sph_ctx* c, long long* count) {
   return SPH_OK;
 }
 
+const char* sph_phase_name(int k) {
+  static const char* names[SPH_NUM_PHASES] = {"vv1",           "hash",    "sort",  "reorder",
+                                              "lists",         "colloid_cells", "density",
+                                              "pairs",         "walls",   "colloids", "vv2"};
+  return (k >= 0 && k < SPH_NUM_PHASES) ? names[k] : "";
+}
+
+sph_status sph_profile_phases(sph_ctx* c, int nsteps, double* ms) {
+  CTX_GUARD(c);
+  if (!ms || nsteps <= 0) return SPH_ERR_STATE;
+  if (!c->initial_done) {
+    sph_status s = do_initial(c);
+    if (s != SPH_OK) return s;
+  }
+  cudaEvent_t ev[SPH_NUM_PHASES + 1];
+  for (auto& e : ev) cudaEventCreate(&e);
+  std::vector<double> acc(SPH_NUM_PHASES, 0.0);
+  bool ext = false, pairs = false;
+  for (const HostBox& hb : c->boxes) {
+    ext = ext || hb.p.ext_force_type != 0;
+    pairs = pairs || hb.p.N_colloids >= 2;
+  }
+  int bad = 0;
+  for (int s = 0; s < nsteps && !bad; ++s) {
+    Launch L = launcher(c);
+    cudaEventRecord(ev[0], c->stream);
+    bad |= launch_vv1_colloids(L) | launch_vv1_particles(L);
+    c->forces_live = false;
+    cudaEventRecord(ev[1], c->stream);
+    bad |= launch_hash(L);
+    cudaEventRecord(ev[2], c->stream);
+    bad |= launch_sort(L, c->key_bits, c->sort);
+    cudaEventRecord(ev[3], c->stream);
+    bad |= launch_reorder(L, false);
+    swap_state(c, false);
+    L = launcher(c);
+    cudaEventRecord(ev[4], c->stream);
+    bad |= launch_build_lists_dim(L, c->dim);
+    cudaEventRecord(ev[5], c->stream);
+    if (c->d.ncoll > 0) bad |= launch_colloid_cells_n(L, c->nboxes, c->max_coll);
+    bad |= launch_advance_time(L, 0);
+    cudaEventRecord(ev[6], c->stream);
+    Launch Lf = L;
+    Lf.d.gradv = nullptr;
+    bad |= launch_density_dim(Lf, c->dim);
+    cudaEventRecord(ev[7], c->stream);
+    bad |= launch_pairs_dim(Lf, c->dim, kPairFused, ext ? 1 : 0);
+    cudaEventRecord(ev[8], c->stream);
+    bad |= launch_wall_forces(Lf);
+    cudaEventRecord(ev[9], c->stream);
+    bad |= launch_colloid_forces(Lf, pairs ? 1 : 0);
+    cudaEventRecord(ev[10], c->stream);
+    bad |= launch_vv2(L) | launch_count_step(L);
+    cudaEventRecord(ev[11], c->stream);
+    cudaEventSynchronize(ev[11]);
+    for (int k = 0; k < SPH_NUM_PHASES; ++k) {
+      float t = 0.f;
+      cudaEventElapsedTime(&t, ev[k], ev[k + 1]);
+      acc[k] += t;
+    }
+    c->host_step++;
+  }
+  for (auto& e : ev) cudaEventDestroy(e);
+  c->forces_live = true;
+  c->pos_dirty = false;
+  drop_graphs(c);  // the buffer parity may have changed
+  if (bad) return cuda_fail(c, "profile_phases");
+  for (int k = 0; k < SPH_NUM_PHASES; ++k) ms[k] = acc[k] / nsteps;
+  return check_device(c);
+}
+
 // ---- state access ----
 sph_status sph_read_field_device(sph_ctx* c, int field, double* dev_out) {
   CTX_GUARD(c);

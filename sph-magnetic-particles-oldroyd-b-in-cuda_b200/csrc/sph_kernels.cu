@@ -78,35 +78,52 @@ __device__ __forceinline__ void min_image(T& rx, T& ry, T& rz, const T L[3], con
 // (kernel_cell_ranges.cu:20-23) or the position is not finite.
 __device__ __forceinline__ int hash_cell(const BoxParams& p, double x, double y, double z) {
   if (!isfinite(x) || !isfinite(y) || (p.dim == 3 && !isfinite(z))) return -2;
-  int cx = (int)floor(x / p.cell_size[0]);
+  const double fx = floor(x / p.cell_size[0]);
+  const double fy = p.wall == 0 ? floor(y / p.cell_size[1])
+                                : floor((y + p.wall_width) / p.cell_size[1]);
+  const double fz = p.dim == 3 ? floor(z / p.cell_size[2]) : 0.0;
+  // far outside the grid: the linear index below would overflow int
+  const double big = 1 << 20;
+  if (fabs(fx) > big || fabs(fy) > big || fabs(fz) > big) return -1;
+  int cx = (int)fx;
   if (cx == p.Ncells[0]) cx = cx - 1;
-  int cy;
-  if (p.wall == 0) {
-    cy = (int)floor(y / p.cell_size[1]);
-    if (cy == p.Ncells[1]) cy = cy - 1;
-  } else {
-    cy = (int)floor((y + p.wall_width) / p.cell_size[1]);
-  }
-  int c;
+  int cy = (int)fy;
+  if (p.wall == 0 && cy == p.Ncells[1]) cy = cy - 1;
+  long long c;
   if (p.dim == 3) {
-    int cz = (int)floor(z / p.cell_size[2]);
+    int cz = (int)fz;
     if (cz == p.Ncells[2]) cz = cz - 1;
-    c = cz * p.Ncells[0] * p.Ncells[1] + cy * p.Ncells[0] + cx;
+    c = (long long)cz * p.Ncells[0] * p.Ncells[1] + (long long)cy * p.Ncells[0] + cx;
   } else {
-    c = cy * p.Ncells[0] + cx;
+    c = (long long)cy * p.Ncells[0] + cx;
   }
   if (c < 0 || c > p.Ntotal_cells - 1) return -1;
-  return c;
+  return (int)c;
 }
 
 // The cell the pair kernels of the reference iterate around: unclamped floor
-// (kernel_densities.cu:52-60).
-__device__ __forceinline__ void own_cell(const BoxParams& p, double x, double y, double z,
+// (kernel_densities.cu:52-60).  Returns false, leaving the outputs untouched, when the
+// position is not finite or so far outside the box that one periodic wrap of the
+// neighbour cells cannot bring them back into the grid; every cell index derived from a
+// true result is in range.
+__device__ __forceinline__ bool own_cell(const BoxParams& p, double x, double y, double z,
                                          int& cx, int& cy, int& cz) {
-  cx = (int)floor(x / p.cell_size[0]);
-  cy = p.wall == 0 ? (int)floor(y / p.cell_size[1])
-                   : (int)floor((y + p.wall_width) / p.cell_size[1]);
-  cz = p.dim == 3 ? (int)floor(z / p.cell_size[2]) : 0;
+  const double fx = floor(x / p.cell_size[0]);
+  const double fy = p.wall == 0 ? floor(y / p.cell_size[1])
+                                : floor((y + p.wall_width) / p.cell_size[1]);
+  const double fz = p.dim == 3 ? floor(z / p.cell_size[2]) : 0.0;
+  // comparisons with NaN are false, so NaN fails every range test
+  if (!(fx >= 1.0 - p.Ncells[0] && fx <= 2.0 * p.Ncells[0] - 2.0)) return false;
+  if (p.wall == 0) {
+    if (!(fy >= 1.0 - p.Ncells[1] && fy <= 2.0 * p.Ncells[1] - 2.0)) return false;
+  } else if (!(fy >= -2.0 * p.Ncells[1] && fy <= 3.0 * p.Ncells[1])) {
+    return false;  // wall axis: out-of-grid rows are skipped, only int overflow matters
+  }
+  if (p.dim == 3 && !(fz >= 1.0 - p.Ncells[2] && fz <= 2.0 * p.Ncells[2] - 2.0)) return false;
+  cx = (int)fx;
+  cy = (int)fy;
+  cz = (int)fz;
+  return true;
 }
 
 __device__ __forceinline__ void raise_status(const Dev& d, unsigned bit, int info) {
@@ -414,15 +431,21 @@ __global__ void __launch_bounds__(kListWarps * 32) k_build_lists(Dev d) {
     const int i = t0 + lane;
     const bool active = i < end;
     float xi = 0.f, yi = 0.f, zi = 0.f;
-    bool odd = false;
+    bool odd = false, lost = false;
     if (active) {
       double4 x = d.pos[i];
       xi = (float)(x.x - ox);
       yi = (float)(x.y - oy);
       zi = (float)(x.z - oz);
-      int ax, ay, az;
-      own_cell(p, x.x, x.y, x.z, ax, ay, az);
-      odd = (ax != cx) || (ay != cy) || (DIM == 3 && az != cz);
+      int ax = 0, ay = 0, az = 0;
+      if (own_cell(p, x.x, x.y, x.z, ax, ay, az)) {
+        odd = (ax != cx) || (ay != cy) || (DIM == 3 && az != cz);
+      } else {
+        // not finite or far outside the box: already reported by the hash; no neighbours
+        lost = true;
+        const bool finite = isfinite(x.x) && isfinite(x.y) && isfinite(x.z);
+        raise_status(d, finite ? kStatCellRange : kStatNaN, d.gid[i]);
+      }
     }
     int cnt = 0;
     for (int ddx = -1; ddx <= 1; ++ddx)
@@ -452,7 +475,7 @@ __global__ void __launch_bounds__(kListWarps * 32) k_build_lists(Dev d) {
             }
             __syncwarp();
             const int n = min(32, e - c0 + 1);
-            if (active && !odd) {
+            if (active && !odd && !lost) {
               for (int q = 0; q < n; ++q) {
                 const float4 c = stage[w][q];
                 const float rx = xi - c.x, ry = yi - c.y;
@@ -481,8 +504,8 @@ __global__ void __launch_bounds__(kListWarps * 32) k_build_lists(Dev d) {
       odd_mask &= odd_mask - 1;
       const int ti = t0 + l;
       const double4 xt = d.pos[ti];
-      int ax, ay, az;
-      own_cell(p, xt.x, xt.y, xt.z, ax, ay, az);
+      int ax = 0, ay = 0, az = 0;
+      if (!own_cell(p, xt.x, xt.y, xt.z, ax, ay, az)) continue;  // checked above: cannot fail
       const double tox = ax * p.cell_size[0];
       const double toy = ay * p.cell_size[1] - (p.wall ? p.wall_width : 0.0);
       const double toz = DIM == 3 ? az * p.cell_size[2] : 0.0;
@@ -1186,9 +1209,16 @@ __global__ void __launch_bounds__(kRedThreads) k_collect_colloids(Dev d) {
 __device__ __forceinline__ int coll_neigh_cells(const BoxParams& p, double x, double y,
                                                 double z, int* cells) {
   const int* Nc = p.Ncells_colloids;
-  const int cxi = (int)floor(x / p.cell_colloids_size[0]);
-  const int cyi = (int)floor(y / p.cell_colloids_size[1]);
-  const int czi = p.dim == 3 ? (int)floor(z / p.cell_colloids_size[2]) : 0;
+  const double fx = floor(x / p.cell_colloids_size[0]);
+  const double fy = floor(y / p.cell_colloids_size[1]);
+  const double fz = p.dim == 3 ? floor(z / p.cell_colloids_size[2]) : 0.0;
+  // a colloid centre that is not finite or lies beyond one periodic image has no
+  // neighbour cells (every index built below then stays inside the coarse grid)
+  if (!(fx >= 1.0 - Nc[0] && fx <= 2.0 * Nc[0] - 2.0)) return 0;
+  if (!(fy >= -2.0 * Nc[1] && fy <= 3.0 * Nc[1])) return 0;
+  if (p.wall == 0 && !(fy >= 1.0 - Nc[1] && fy <= 2.0 * Nc[1] - 2.0)) return 0;
+  if (p.dim == 3 && !(fz >= 1.0 - Nc[2] && fz <= 2.0 * Nc[2] - 2.0)) return 0;
+  const int cxi = (int)fx, cyi = (int)fy, czi = (int)fz;
   int n = 0;
   const int dz0 = p.dim == 3 ? -1 : 0, dz1 = p.dim == 3 ? 1 : 0;
   for (int dx = -1; dx <= 1; ++dx)

@@ -48,7 +48,8 @@ EXPORTS = [
     "sph_step", "sph_synchronize", "sph_read_field", "sph_write_field",
     "sph_read_field_device", "sph_read_type", "sph_read_colloid_field",
     "sph_read_wall_forces", "sph_export_cells", "sph_export_colloid_cells",
-    "sph_kinetic_energy", "sph_last_step_ms", "sph_kernel_launches",
+    "sph_kinetic_energy", "sph_last_step_ms", "sph_kernel_launches", "sph_host_setup",
+    "sph_profile_phases", "sph_phase_name",
 ]
 
 c_int, c_double, c_void_p, c_char_p = ctypes.c_int, ctypes.c_double, ctypes.c_void_p, ctypes.c_char_p
@@ -157,6 +158,53 @@ def read_input(path):
     if st != 0:
         raise SphError(st, msg.value.decode())
     return inp, coll
+
+
+class SphHostState(ctypes.Structure):
+    _fields_ = [(n, PD) for n in ["x", "y", "z", "vx", "vy", "vz", "mass", "cxx", "cxy", "cyy",
+                                  "cxz", "cyz", "czz"]] + [
+        ("type", PI), ("walls_list", PI), ("walls_start", PI), ("colloids_list", PI),
+        ("colloids_start", PI), ("x_center", PD), ("y_center", PD), ("z_center", PD)]
+
+
+def host_setup(input_path, particles_path=None):
+    """Initial state as the engine's host set-up builds it (no GPU needed): the arrays the
+    reference's class_system holds on the host after constructor + initialize."""
+    L = lib()
+    L.sph_host_setup.argtypes = [ctypes.POINTER(SphInput), c_char_p, c_int,
+                                 ctypes.POINTER(SphHostState), PI, ctypes.POINTER(SphInfo)]
+    inp, coll = read_input(str(input_path))
+    inp.coll_xyz = coll.ctypes.data_as(PD)
+    pp = particles_path.encode() if particles_path else None
+    n = c_int(0)
+    info = SphInfo()
+    st = L.sph_host_setup(ctypes.byref(inp), pp, 0, None, ctypes.byref(n), ctypes.byref(info))
+    if st != 0:
+        raise SphError(st, "sph_host_setup failed (see stderr)")
+    cap = max(n.value, 1)
+    out = {k: np.zeros(cap) for k in ["x", "y", "z", "vx", "vy", "vz", "mass", "cxx", "cxy",
+                                     "cyy", "cxz", "cyz", "czz", "x_center", "y_center", "z_center"]}
+    for k in ["type", "walls_list", "colloids_list", "colloids_start"]:
+        out[k] = np.zeros(cap, dtype=np.int32)
+    out["walls_start"] = np.zeros(2, dtype=np.int32)
+    hs = SphHostState()
+    for name, typ in SphHostState._fields_:
+        setattr(hs, name, out[name].ctypes.data_as(typ))
+    st = L.sph_host_setup(ctypes.byref(inp), pp, cap, ctypes.byref(hs), ctypes.byref(n), ctypes.byref(info))
+    if st != 0:
+        raise SphError(st, "sph_host_setup failed (see stderr)")
+    res = {}
+    for name, _ in SphInfo._fields_:
+        v = getattr(info, name)
+        res[name] = list(v) if isinstance(v, ctypes.Array) else v
+    N, nl, nw, nc = info.N, info.Nlist_colloids, info.Nlist_walls, info.N_colloids
+    arrays = {k: out[k][:N] for k in ["x", "y", "z", "vx", "vy", "vz", "mass", "cxx", "cxy",
+                                     "cyy", "cxz", "cyz", "czz", "type"]}
+    arrays.update(walls_list=out["walls_list"][:nw], walls_start=out["walls_start"],
+                  colloids_list=out["colloids_list"][:nl], colloids_start=out["colloids_start"][:nc],
+                  x_center=out["x_center"][:nl], y_center=out["y_center"][:nl],
+                  z_center=out["z_center"][:nl])
+    return arrays, res
 
 
 class System:
@@ -272,6 +320,17 @@ class System:
         v = ctypes.c_longlong()
         self._ok(lib().sph_kernel_launches(self._h, ctypes.byref(v)))
         return v.value
+
+    def profile_phases(self, nsteps=5):
+        """Mean device milliseconds per phase of a step (CUDA events on the engine's stream)."""
+        L = lib()
+        L.sph_profile_phases.argtypes = [c_void_p, c_int, PD]
+        L.sph_phase_name.argtypes = [c_int]
+        L.sph_phase_name.restype = c_char_p
+        n = 11
+        out = np.zeros(n)
+        self._ok(L.sph_profile_phases(self._h, int(nsteps), out.ctypes.data_as(PD)))
+        return {L.sph_phase_name(k).decode(): float(out[k]) for k in range(n)}
 
     # --- state ---
     def field(self, name):

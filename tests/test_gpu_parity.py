@@ -1,0 +1,319 @@
+"""Parity of the CUDA engine (through its C ABI) with the FP64 oracle and with the
+reference build's golden dumps.
+
+Tolerances (max |engine - oracle| / scale of the field group, see conftest.GROUPS):
+  FP64 engine  : 1e-10 for every group; integer cell / sort arrays bit-exact.
+  mixed engine : pair arithmetic in float; states (positions, conformation tensor,
+                 density, velocities) within 2e-5 and forces / dc/dt within 5e-5 after 5
+                 steps.  Two quantities that are small residuals of large cancelling
+                 float terms get a stated wider bound: forces and velocities of a fluid
+                 at rest on a perfect lattice (Kolmogorov start, 5e-3) and colloid torques
+                 and angular velocities (2e-3).
+"""
+import os
+
+import numpy as np
+import pytest
+
+import make_golden as mg
+import oracle
+import sph_b200
+import sph_input
+from conftest import COLLOID_GROUPS, GROUPS, group_error
+
+pytestmark = pytest.mark.gpu
+HERE = os.path.dirname(os.path.abspath(__file__))
+INTS = ["particle_cell", "particle_index", "cell_start", "cell_end"]
+
+MIXED_TOL = dict(pos=1e-9, conf=1e-8, dens=2e-5, press=2e-5, vel=2e-5, force=5e-5, dcdt=5e-5,
+                 grad=5e-5, cpos=1e-9, cvel=2e-5, comega=2e-3, cforce=5e-5, ctorque=2e-3,
+                 walls=2e-5)
+MIXED_WIDE = {"kolmogorov2d": dict(vel=5e-3, force=5e-3, dcdt=5e-3)}
+
+
+def open_case(name, workdir, precision="fp64", use_graph=True):
+    mg.case_dir(name, workdir)
+    pp = os.path.join(workdir, "input_particles.in")
+    pp = pp if os.path.exists(pp) else None
+    inp = os.path.join(workdir, "input")
+    e = sph_b200.System(inp, [pp] if pp else None, precision=precision, use_graph=use_graph)
+    return e, oracle.Oracle(inp, pp)
+
+
+def compare_state(e, o, tol, label, skip=()):
+    dim = o.info()["dim"]
+    errs = {}
+    for gname, (fields, norm) in GROUPS.items():
+        if gname in skip or gname == "grad":
+            continue
+        errs[gname] = group_error(e.field, o.field, fields, norm, dim)
+    if o.info()["N_colloids"]:
+        for gname, (fields, norm) in COLLOID_GROUPS.items():
+            errs[gname] = group_error(e.colloid_field, o.field, fields, norm, dim)
+    if o.info()["wall"]:
+        wf = e.wall_forces()[0]
+        ref = np.stack([o.field("fx_wall"), o.field("fy_wall"), o.field("fz_wall")], axis=1)
+        if dim == 2:
+            wf, ref = wf[:, :2], ref[:, :2]
+        errs["walls"] = float(np.abs(wf - ref).max() / max(np.abs(ref).max(), 1e-300))
+    for k, v in errs.items():
+        t = tol if isinstance(tol, float) else tol[k]
+        assert v <= t, (label, k, v, t)
+    return errs
+
+
+@pytest.mark.parametrize("name", list(mg.CASES))
+def test_fp64_engine_matches_oracle(name, workdir):
+    e, o = open_case(name, workdir)
+    o.run(0)
+    e.step(0)
+    compare_state(e, o, 1e-10, "step0")
+    cells = e.export_cells()
+    for k in INTS:
+        assert np.array_equal(cells[k], o.ifield(k)), k
+    o.run(5)
+    e.step(5)
+    e.synchronize()
+    compare_state(e, o, 1e-10, "step5")
+    cells = e.export_cells()
+    for k in INTS:
+        assert np.array_equal(cells[k], o.ifield(k)), k
+    if o.info()["N_colloids"] >= 2:
+        cc = e.export_colloid_cells()
+        for k in ["coll_cell", "coll_index", "coll_cell_start", "coll_cell_end"]:
+            assert np.array_equal(cc[k], o.ifield(k)), k
+    assert e.kernel_launches() > 0
+
+
+@pytest.mark.parametrize("name", list(mg.CASES))
+def test_mixed_engine_matches_oracle(name, workdir):
+    e, o = open_case(name, workdir, precision="mixed")
+    tol = dict(MIXED_TOL)
+    tol.update(MIXED_WIDE.get(name, {}))
+    o.run(0)
+    e.step(0)
+    compare_state(e, o, tol, "step0")
+    o.run(5)
+    e.step(5)
+    e.synchronize()
+    compare_state(e, o, tol, "step5")
+
+
+@pytest.mark.parametrize("name", list(mg.CASES))
+def test_engine_matches_reference_build(name, workdir):
+    """Engine against the reference's own CUDA build (golden dumps)."""
+    g = np.load(os.path.join(HERE, "golden", name + ".npz"))
+    e, _ = open_case(name, workdir)
+    dim = e.info()["dim"]
+    steps = [0] if name == "colloids3d" else mg.STEPS
+    done = 0
+    for s in steps:
+        e.step(s - done)
+        e.synchronize()
+        done = s
+        keys = {k[len("s%d_" % s):] for k in g.files if k.startswith("s%d_" % s)}
+        cells = e.export_cells()
+        for k in INTS:
+            assert np.array_equal(cells[k], g["s%d_%s" % (s, k)]), (s, k)
+        for gname, (fields, norm) in GROUPS.items():
+            fl = [f for f in fields if f in keys]
+            if not fl or gname == "grad":
+                continue
+            err = group_error(e.field, lambda f: g["s%d_%s" % (s, f)], fl, norm, dim)
+            assert err <= 1e-10, (s, gname, err)
+
+
+def test_class_system_methods_step_by_step(workdir):
+    """The step methods called one by one, in the order of main.cu:358-467, against the
+    oracle after every method (colloids, walls and a body force all active)."""
+    e, o = open_case("colloids2d", workdir, use_graph=False)
+    tol = 1e-10
+    dim = 2
+
+    def check(fields, label, norm="max"):
+        err = group_error(e.field, o.field, fields, norm, dim)
+        assert err <= tol, (label, err)
+
+    e.neighbours_search()
+    o.neighbours_search()
+    cells = e.export_cells()
+    for k in INTS:
+        assert np.array_equal(cells[k], o.ifield(k))
+    for step in range(3):
+        t = o.info()["t0"] + o.info()["dt"] * step
+        m = o.magnetic_moment(t)
+        if step > 0:
+            e.V_Verlet_step1()
+            o.vv_step1()
+            check(["x", "y"], "vv1 pos", "unit")
+            check(["vx", "vy"], "vv1 vel")
+            e.neighbours_search()
+            o.neighbours_search()
+            cells = e.export_cells()
+            for k in INTS:
+                assert np.array_equal(cells[k], o.ifield(k))
+        e.calculate_density()
+        o.calculate_density()
+        check(["dens"], "density")
+        e.calculate_pressure()
+        o.calculate_pressure()
+        check(["press"], "pressure")
+        e.calculate_vel_gradient()
+        o.calculate_vel_gradient()
+        check(["gxx", "gxy", "gyx", "gyy"], "vel_gradient (all particles)")
+        e.calculate_forces(m)
+        o.calculate_forces(m)
+        check(["fx", "fy"], "forces")
+        check(["dcdt_xx", "dcdt_xy", "dcdt_yy"], "dcdt")
+        for f in ["fx_colloid", "fy_colloid", "tz_colloid"]:
+            a, b = e.colloid_field(f), o.field(f)
+            assert np.abs(a - b).max() <= tol * np.abs(b).max(), f
+        wf = e.wall_forces()[0]
+        assert np.abs(wf[:, 0] - o.field("fx_wall")).max() <= tol * np.abs(o.field("fx_wall")).max()
+        if step > 0:
+            e.V_Verlet_step2()
+            o.vv_step2()
+            check(["vx", "vy"], "vv2 vel")
+            check(["cxx", "cxy", "cyy"], "vv2 conf", "unit")
+    ke = e.kinetic_energy()[0]
+    assert ke == pytest.approx(o.kinetic_energy(), rel=1e-12)
+
+
+def test_device_errors_are_reported_not_trapped(workdir):
+    """A non-finite position and a particle outside the wall band come back as statuses;
+    the context keeps working once the state is repaired."""
+    e, _ = open_case("couette2d", workdir)
+    e.step(1)
+    e.synchronize()
+    x = e.field("x")
+    bad = x.copy()
+    bad[10] = np.nan
+    e.set_field("x", bad)
+    with pytest.raises(sph_b200.SphError) as err:
+        e.neighbours_search()
+    assert err.value.status == "SPH_ERR_NAN"
+    e.set_field("x", x)
+    y = e.field("y")
+    bad = y.copy()
+    bad[5] = -0.5  # far below the bottom wall layers: hashes outside the grid
+    e.set_field("y", bad)
+    with pytest.raises(sph_b200.SphError) as err:
+        e.neighbours_search()
+    assert err.value.status == "SPH_ERR_CELL_RANGE"
+    e.set_field("y", y)
+    e.neighbours_search()
+    e.step(2)
+    e.synchronize()
+
+
+@pytest.mark.parametrize("precision", ["fp64", "mixed"])
+def test_bitwise_reproducible(precision, workdir):
+    out = []
+    for k in range(2):
+        e, _ = open_case("colloids2d", workdir, precision=precision)
+        e.step(10)
+        e.synchronize()
+        out.append(np.concatenate([e.field(f) for f in ["x", "y", "vx", "vy", "fx", "cxy"]] +
+                                  [e.colloid_field("coll_x"), e.wall_forces().ravel()]))
+        e.close()
+    assert np.array_equal(out[0], out[1])
+
+
+def test_graph_and_direct_paths_agree(workdir):
+    a, _ = open_case("couette3d", workdir, use_graph=True)
+    b, _ = open_case("couette3d", workdir, use_graph=False)
+    a.step(4)
+    b.step(4)
+    a.synchronize()
+    b.synchronize()
+    for f in ["x", "vx", "fy", "cxy", "dens"]:
+        assert np.array_equal(a.field(f), b.field(f)), f
+
+
+def test_ensemble_equals_single_boxes(workdir):
+    """Boxes of different sizes and parameters in one context give, box by box, the same
+    bits as each box run alone."""
+    specs = [
+        dict(N=(32, 32), L=(1.0, 1.0), dim=2, overlap=4.0, wall=1, Vwall_top=0.3,
+             Vwall_bottom=-0.3, dt=2e-5, tau=0.5),
+        dict(N=(48, 40), L=(1.2, 1.0), dim=2, overlap=4.0, wall=1, Vwall_top=0.1,
+             Vwall_bottom=-0.1, dt=2e-5, tau=2.0, N_colloids=2, coll_R=4.0 / 40,
+             coll_x=((0.3, 0.5), (0.8, 0.45)), tau_repulsion=5.0, cutoff_magnetic=0.3,
+             F0_magnetic=1e-4, F0_repulsion=1e-3, omega_magnetic=3.0),
+        dict(N=(40, 40), L=(1.0, 1.0), dim=2, overlap=4.0, wall=0, ext_force_type=2,
+             ext_force=(1.0, 0.0), dt=5e-5),
+    ]
+    paths = []
+    for k, s in enumerate(specs):
+        p = os.path.join(workdir, "input%d" % k)
+        sph_input.write_input(p, **s)
+        paths.append(p)
+    ens = sph_b200.System(paths)
+    ens.step(6)
+    ens.synchronize()
+    off = 0
+    for k, p in enumerate(paths):
+        one = sph_b200.System(p)
+        one.step(6)
+        one.synchronize()
+        n = one.N
+        for f in ["x", "y", "vx", "vy", "fx", "dens", "cxy"]:
+            assert np.array_equal(ens.field(f)[off:off + n], one.field(f)), (k, f)
+        assert np.array_equal(ens.wall_forces()[k], one.wall_forces()[0])
+        assert ens.kinetic_energy()[k] == one.kinetic_energy()[0]
+        off += n
+        one.close()
+
+
+def test_momentum_conserved_periodic(workdir):
+    """Pair forces are antisymmetric: without walls, colloids or body force the total
+    momentum stays at its initial value to rounding (kernel_forces.cu:429-440)."""
+    spec = dict(N=(20, 20, 20), L=(1.0, 1.0, 1.0), dim=3, overlap=3.0, dt=2e-5)
+    p0 = os.path.join(workdir, "input0")
+    sph_input.write_input(p0, **spec)
+    o = oracle.Oracle(p0)
+    n = o.info()["N"]
+    rng = np.random.default_rng(3)
+    v = rng.uniform(-0.01, 0.01, size=(3, n))
+    pp = os.path.join(workdir, "input_particles.in")
+    sph_input.write_particles(pp, 3, o.field("x"), o.field("y"), o.field("z"), v[0], v[1], v[2],
+                              o.field("mass"), o.ifield("type"), o.field("cxx"), o.field("cxy"),
+                              o.field("cyy"), o.field("cxz"), o.field("cyz"), o.field("czz"))
+    path = os.path.join(workdir, "input")
+    sph_input.write_input(path, **dict(spec, new_sim=1))
+    e = sph_b200.System(path, [pp])
+    m = e.field("mass")
+    p_init = np.array([np.sum(m * e.field(f)) for f in ["vx", "vy", "vz"]])
+    e.step(20)
+    e.synchronize()
+    p_end = np.array([np.sum(m * e.field(f)) for f in ["vx", "vy", "vz"]])
+    scale = np.sum(m * np.abs(e.field("vx")))
+    assert np.abs(p_end - p_init).max() <= 1e-12 * scale
+
+
+def test_full_size_couette_128(workdir):
+    """The 128^3 Couette workload (2,195,456 particles): a few steps without errors, the
+    lattice neighbourhood of 92 neighbours, FP64 and mixed within the mixed tolerance."""
+    spec = dict(N=(128, 128, 128), L=(1.0, 1.0, 1.0), dim=3, overlap=3.0, wall=1,
+                Vwall_bottom=-0.5, Vwall_top=0.5, dt=2e-5)
+    path = os.path.join(workdir, "input")
+    sph_input.write_input(path, **spec)
+    a = sph_b200.System(path, precision="fp64")
+    assert a.N == 128 * 134 * 128
+    a.step(0)
+    cells = a.export_cells()
+    assert np.all(np.bincount(cells["particle_cell"], minlength=42 * 44 * 42) > 0)
+    d = a.field("dens")
+    t = a.type()
+    assert np.ptp(d[t == 0][:1000]) < 1e-9 * d.mean()
+    a.step(3)
+    a.synchronize()
+    b = sph_b200.System(path, precision="mixed")
+    b.step(3)
+    b.synchronize()
+    for gname in ["pos", "conf", "vel", "dens"]:
+        fields, norm = GROUPS[gname]
+        err = group_error(b.field, a.field, fields, norm, 3)
+        assert err <= MIXED_TOL[gname], (gname, err)
+    wa, wb = a.wall_forces(), b.wall_forces()
+    assert np.abs(wa - wb).max() <= 2e-5 * np.abs(wa).max()
