@@ -240,6 +240,34 @@ sph_status sph_last_step_ms(sph_ctx* ctx, double* ms);
 /* Launch counters: kernels launched by the engine since creation. */
 sph_status sph_kernel_launches(const sph_ctx* ctx, long long* count);
 
+/* Neighbour search that allocates nothing.  No counterpart in the reference (whose
+   thrust-based search allocates temporary storage on every call); it is for callers
+   that cannot call cudaMalloc, such as programs whose device memory is reserved up front
+   by their own allocator, or time loops that must not let an allocation stall the
+   device.  Same results as sph_neighbours_search / sph_export_cells for one box, on
+   caller-owned device arrays in original particle order: x, y (and z in 3D) hold n
+   positions; particle_cell and particle_index (n ints) receive the (cell, id)-sorted
+   pairs; cell_start and cell_end (Ncells[0]*Ncells[1]*Ncells[2] ints) are written for
+   occupied cells only and keep earlier values elsewhere, as the reference's arrays do.
+   The sort's scratch is a static device array of the library sized for at most
+   SPH_NOALLOC_MAX_PARTICLES particles (about 13 MB, held by every GPU that loads the
+   library until the process exits); larger n returns SPH_ERR_CAPACITY.  The first call
+   on a device looks up that array's device address (once per device).  All calls share
+   the array: calls that overlap on the GPU race, so serialise them.  The call runs on
+   `stream` (a cudaStream_t, NULL for the default stream) and waits for it before it
+   returns; a particle outside the grid gives SPH_ERR_CELL_RANGE. */
+#define SPH_NOALLOC_MAX_PARTICLES (1 << 20)
+typedef struct sph_grid {
+  int dim, wall;
+  int Ncells[3];
+  double cell_size[3];
+  double wall_width;
+} sph_grid;
+sph_status sph_neighbours_search_noalloc(const double* x, const double* y, const double* z,
+                                         int n, const sph_grid* grid, int* particle_cell,
+                                         int* particle_index, int* cell_start, int* cell_end,
+                                         void* stream);
+
 /* Profiling (no reference counterpart; the reference times with clock(), main.cu:381-427):
    runs nsteps full steps with CUDA events between the phases on the context's stream and
    writes the mean device time of each phase in milliseconds to ms[0..SPH_NUM_PHASES-1]. */

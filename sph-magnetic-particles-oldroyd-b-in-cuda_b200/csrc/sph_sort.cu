@@ -214,4 +214,45 @@ int launch_sort(const Launch& L, int key_bits, const SortScratch& scr) {
   return 0;
 }
 
+// The same sort on caller-provided buffers: keys_in (n keys, values are the indices
+// 0..n-1), outputs keys_out / vals_out, ping-pong buffers keys_tmp / vals_tmp and a
+// histogram of sort_hist_len(n, key_bits) ints.  Used by the allocation-free neighbour
+// search (sph_noalloc.cu).
+int launch_sort_buffers(const int* keys_in, int n, int key_bits, int* keys_out, int* vals_out,
+                        int* keys_tmp, int* vals_tmp, int* hist, void* stream,
+                        long long* launches) {
+  if (n == 0) return 0;
+  cudaStream_t st = static_cast<cudaStream_t>(stream);
+  if (key_bits < 1) key_bits = 1;
+  const int passes = (key_bits + kMaxBits - 1) / kMaxBits;
+  const int bits = (key_bits + passes - 1) / passes;
+  const int ntiles = (n + kTile - 1) / kTile;
+  const int m = (1 << bits) * ntiles;
+  const int nchunks = (m + kScanChunk - 1) / kScanChunk;
+  int* sums = hist + (size_t)kMaxBuckets * ntiles;
+  const int* kin = keys_in;
+  const int* vin = nullptr;
+  for (int pass = 0; pass < passes; ++pass) {
+    const bool last_even = ((passes - 1 - pass) % 2) == 0;
+    int* kout = last_even ? keys_out : keys_tmp;
+    int* vout = last_even ? vals_out : vals_tmp;
+    const int shift = pass * bits;
+    k_radix_hist<<<ntiles, kThreads, 0, st>>>(kin, n, shift, bits, ntiles, hist);
+    k_scan_sums<<<nchunks, kThreads, 0, st>>>(hist, m, sums);
+    k_scan_top<<<1, kThreads, 0, st>>>(sums, nchunks);
+    k_scan_apply<<<nchunks, kThreads, 0, st>>>(hist, m, sums);
+    k_radix_scatter<<<ntiles, kThreads, 0, st>>>(kin, vin, n, shift, bits, ntiles, hist, kout,
+                                                 vout);
+    if (launches) *launches += 5;
+    const cudaError_t e = cudaGetLastError();
+    if (e != cudaSuccess) {
+      last_launch_error() = (int)e;
+      return 1;
+    }
+    kin = kout;
+    vin = vout;
+  }
+  return 0;
+}
+
 }  // namespace sph

@@ -207,6 +207,23 @@ def host_setup(input_path, particles_path=None):
     return arrays, res
 
 
+class SphGrid(ctypes.Structure):
+    _fields_ = [("dim", c_int), ("wall", c_int), ("Ncells", c_int * 3),
+                ("cell_size", c_double * 3), ("wall_width", c_double)]
+
+
+def neighbours_search_noalloc(x, y, z, n, grid, particle_cell, particle_index, cell_start,
+                              cell_end, stream=None):
+    """Allocation-free neighbour search on caller-owned device arrays (device pointers as
+    ints).  For callers that cannot allocate device memory; returns the raw status code."""
+    L = lib()
+    L.sph_neighbours_search_noalloc.argtypes = [c_void_p, c_void_p, c_void_p, c_int,
+                                                ctypes.POINTER(SphGrid), c_void_p, c_void_p,
+                                                c_void_p, c_void_p, c_void_p]
+    return L.sph_neighbours_search_noalloc(x, y, z, int(n), ctypes.byref(grid), particle_cell,
+                                           particle_index, cell_start, cell_end, stream)
+
+
 class System:
     """One or more simulation boxes on the GPU (the reference's class_system)."""
 
