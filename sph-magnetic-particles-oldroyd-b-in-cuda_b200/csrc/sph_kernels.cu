@@ -476,6 +476,9 @@ __global__ void __launch_bounds__(kListWarps * 32) k_build_lists(Dev d) {
             __syncwarp();
             const int n = min(32, e - c0 + 1);
             if (active && !odd && !lost) {
+              // hit mask of this chunk, branch-free; staged candidate q is slot c0 + q
+              unsigned hits = 0u;
+#pragma unroll 4
               for (int q = 0; q < n; ++q) {
                 const float4 c = stage[w][q];
                 const float rx = xi - c.x, ry = yi - c.y;
@@ -484,10 +487,15 @@ __global__ void __launch_bounds__(kListWarps * 32) k_build_lists(Dev d) {
                   const float rz = zi - c.z;
                   r2 += rz * rz;
                 }
-                if (r2 < cut2) {
-                  if (cnt < cap) d.nbr[(size_t)cnt * Np + i] = __float_as_int(c.w);
-                  ++cnt;
-                }
+                hits |= (r2 < cut2 ? 1u : 0u) << q;
+              }
+              // append in candidate order to the particle's own list row
+              int* rowp = d.nbr + (size_t)i * cap;
+              while (hits) {
+                const int q = __ffs(hits) - 1;
+                hits &= hits - 1u;
+                if (cnt < cap) rowp[cnt] = c0 + q;
+                ++cnt;
               }
             }
             __syncwarp();
@@ -545,7 +553,7 @@ __global__ void __launch_bounds__(kListWarps * 32) k_build_lists(Dev d) {
               }
               const unsigned hits = __ballot_sync(SPH_FULL, hit);
               const int pos = tcnt + __popc(hits & ((1u << lane) - 1u));
-              if (hit && pos < cap) d.nbr[(size_t)pos * Np + ti] = j;
+              if (hit && pos < cap) d.nbr[(size_t)ti * cap + pos] = j;
               tcnt += __popc(hits);
             }
           }
@@ -662,15 +670,29 @@ __global__ void k_density(Dev d) {
   const T rcut_inv = (T)p.rcut_inv, cw = (T)p.cw;
   const V xi = P[i];
   const int n = min(d.nbr_cnt[i], d.cap);
-  const int Np = d.Npad;
+  // the particle's list row, read four indices at a time one batch ahead
+  const int4* __restrict__ row = reinterpret_cast<const int4*>(d.nbr + (size_t)i * d.cap);
   T dens = T(0);
-  for (int k = 0; k < n; ++k) {
-    const int j = __ldg(&d.nbr[(size_t)k * Np + i]);
-    const V xj = P[j];
-    T rx = xi.x - xj.x, ry = xi.y - xj.y, rz = DIM == 3 ? xi.z - xj.z : T(0);
-    min_image<T, DIM>(rx, ry, rz, L, h, p.wall);
-    const T r2 = DIM == 3 ? rx * rx + ry * ry + rz * rz : rx * rx + ry * ry;
-    if (r2 < rcutsq) dens = dens + sph_w<T>(sqrt(r2), rcut_inv, cw);
+  int4 nxt = n > 0 ? __ldg(&row[0]) : make_int4(0, 0, 0, 0);
+  for (int k0 = 0; k0 < n; k0 += 4) {
+    const int4 cur = nxt;
+    if (k0 + 4 < n) nxt = __ldg(&row[(k0 >> 2) + 1]);
+    const int m = min(4, n - k0);
+#pragma unroll
+    for (int q = 0; q < 4; ++q) {
+      if (q >= m) break;
+      const int j = q == 0 ? cur.x : q == 1 ? cur.y : q == 2 ? cur.z : cur.w;
+      const V xj = P[j];
+      T rx = xi.x - xj.x, ry = xi.y - xj.y, rz = DIM == 3 ? xi.z - xj.z : T(0);
+      min_image<T, DIM>(rx, ry, rz, L, h, p.wall);
+      const T r2 = DIM == 3 ? rx * rx + ry * ry + rz * rz : rx * rx + ry * ry;
+      if (r2 < rcutsq) {
+        // r = r2 / sqrt(r2) through the reciprocal square root; the particle itself
+        // (r2 = 0) contributes W(0)
+        const T r = r2 > T(0) ? r2 * rsqrt(r2) : T(0);
+        dens = dens + sph_w<T>(r, rcut_inv, cw);
+      }
+    }
   }
   const double densd = (double)dens;
   d.dens[i] = densd;
@@ -845,7 +867,7 @@ __device__ __forceinline__ void ghost_solid_i(const BoxParams& p, const CollView
 }
 
 template <typename T, int DIM, int MODE, bool EXT>
-__global__ void __launch_bounds__(128) k_pairs(Dev d) {
+__global__ void __launch_bounds__(128, 3) k_pairs(Dev d) {
   using Rec = typename RecOf<T>::type;
   const int i = blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= d.Ntot) return;
@@ -878,9 +900,17 @@ __global__ void __launch_bounds__(128) k_pairs(Dev d) {
     for (int c = 0; c < DIM; ++c) g[a][c] = T(0);
   T f[3] = {T(0), T(0), T(0)};
   const int n = min(d.nbr_cnt[i], d.cap);
-  const int Np = d.Npad;
-  for (int k = 0; k < n; ++k) {
-    const int j = __ldg(&d.nbr[(size_t)k * Np + i]);
+  // the particle's list row, read four indices at a time one batch ahead so that the
+  // index loads overlap the arithmetic of the previous batch
+  const int4* __restrict__ row = reinterpret_cast<const int4*>(d.nbr + (size_t)i * d.cap);
+  int4 nxt = n > 0 ? __ldg(&row[0]) : make_int4(0, 0, 0, 0);
+  for (int k0 = 0; k0 < n; k0 += 4) {
+   const int4 cur = nxt;
+   if (k0 + 4 < n) nxt = __ldg(&row[(k0 >> 2) + 1]);
+   const int m = min(4, n - k0);
+#pragma unroll 1
+   for (int q = 0; q < m; ++q) {
+    const int j = q == 0 ? cur.x : q == 1 ? cur.y : q == 2 ? cur.z : cur.w;
     if (j == i) continue;
     const Rec rj = rec[j];
     const int tj = type_of(rj.tinfo);
@@ -904,8 +934,8 @@ __global__ void __launch_bounds__(128) k_pairs(Dev d) {
     } else {
       ghost_solid_i<T, DIM>(p, cv, ti, coll0, yi, (T)rj.x, (T)rj.y, (T)rj.z, vj, r, L, h, v);
     }
-    const T rr = sqrt(r2);
-    const T rinv = T(1) / rr;
+    const T rinv = rsqrt(r2);  // r and 1/r from one reciprocal square root
+    const T rr = r2 * rinv;
     const T gw = sph_gradw<T>(rr, rcut_inv, c_gradw);
     const T e[3] = {r[0] * rinv, r[1] * rinv, DIM == 3 ? r[2] * rinv : T(0)};
     if (pair_grad) {
@@ -974,6 +1004,7 @@ __global__ void __launch_bounds__(128) k_pairs(Dev d) {
         f[2] += aux1 * v[2] + aux2 * e[2];
       }
     }
+  }
   }
   const int Np2 = d.Npad;
   if (MODE == kPairGradvAll || (MODE == kPairFused && d.gradv != nullptr && do_grad)) {

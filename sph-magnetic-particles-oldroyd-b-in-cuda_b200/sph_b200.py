@@ -17,7 +17,8 @@ import subprocess
 import numpy as np
 
 HERE = os.path.dirname(os.path.abspath(__file__))
-LIB_PATH = os.path.join(HERE, "lib", "libsph_b200.so")
+# SPH_B200_LIB selects another build of the engine library (e.g. a tuning variant)
+LIB_PATH = os.environ.get("SPH_B200_LIB") or os.path.join(HERE, "lib", "libsph_b200.so")
 
 FIELDS = [
     "x", "y", "z", "vx", "vy", "vz", "fx", "fy", "fz", "dens", "press", "mass",
