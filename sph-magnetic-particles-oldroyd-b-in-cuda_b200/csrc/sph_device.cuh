@@ -1,0 +1,548 @@
+// sph_device.cuh -- device helpers shared by the per-particle and the per-cell kernels:
+// the SPH kernel, minimum image, cell checks, neighbour records, Morris ghost velocities
+// and the pair arithmetic of the velocity-gradient / force pass.
+#pragma once
+#include <cuda_runtime.h>
+#include <math.h>
+
+#include "sph_internal.h"
+
+namespace sph {
+#define SPH_FULL 0xffffffffu
+
+__device__ __forceinline__ int type_of(int t) { return t & kTypeMask; }
+__device__ __forceinline__ int box_of(int t) { return t >> kTypeBits; }
+
+template <typename T> struct V4;
+template <> struct V4<double> { using type = double4; };
+template <> struct V4<float> { using type = float4; };
+
+template <typename T> struct RecOf;
+template <> struct RecOf<double> { using type = RecD; };
+template <> struct RecOf<float> { using type = RecF; };
+
+// ---------------------------------------------------------------------------------
+// SPH kernel and its radial derivative (kernel_W.cu:13-59, kernel_gradW.cu:13-53).
+// Written branch-free: the clamped terms are exact zeros where the reference skips
+// them, so the value is the same as the branchy form.
+// ---------------------------------------------------------------------------------
+template <typename T>
+__device__ __forceinline__ T sph_w(T r, T rcut_inv, T cw) {
+  T q3 = (r * rcut_inv) * T(3);
+  T t1 = T(3) - q3, t2 = T(2) - q3, t3 = T(1) - q3;
+  T a1 = t1 * t1, a2 = t2 * t2, a3 = t3 * t3;
+  T w = (a1 * a1) * t1;
+  if (q3 < T(2)) w = w - T(6) * ((a2 * a2) * t2);
+  if (q3 < T(1)) w = w + T(15) * ((a3 * a3) * t3);
+  return cw * w;
+}
+
+template <typename T>
+__device__ __forceinline__ T sph_gradw(T r, T rcut_inv, T c_gradw) {
+  T q3 = T(3) * (r * rcut_inv);
+  T t1 = T(3) - q3, t2 = T(2) - q3, t3 = T(1) - q3;
+  T a1 = t1 * t1, a2 = t2 * t2, a3 = t3 * t3;
+  T g = a1 * a1;
+  if (q3 < T(2)) g = g - T(6) * (a2 * a2);
+  if (q3 < T(1)) g = g + T(15) * (a3 * a3);
+  return c_gradw * g;
+}
+
+// Minimum image as the reference writes it: subtract L above L/2, add L below -L/2
+// (kernel_densities.cu:90-110).  y is periodic only without walls; z only in 3D.
+template <typename T, int DIM>
+__device__ __forceinline__ void min_image(T& rx, T& ry, T& rz, const T L[3], const T h[3],
+                                          int wall) {
+  if (rx > h[0]) rx -= L[0];
+  if (rx < -h[0]) rx += L[0];
+  if (!wall) {
+    if (ry > h[1]) ry -= L[1];
+    if (ry < -h[1]) ry += L[1];
+  }
+  if (DIM == 3) {
+    if (rz > h[2]) rz -= L[2];
+    if (rz < -h[2]) rz += L[2];
+  }
+}
+
+// Cell of a position as kernel_cell_list.cu:15-63 computes it (with its clamp rules).
+// Returns the box-local linear cell, or -1 when the reference would assert
+// (kernel_cell_ranges.cu:20-23) or the position is not finite.
+__device__ __forceinline__ int hash_cell(const BoxParams& p, double x, double y, double z) {
+  if (!isfinite(x) || !isfinite(y) || (p.dim == 3 && !isfinite(z))) return -2;
+  const double fx = floor(x / p.cell_size[0]);
+  const double fy = p.wall == 0 ? floor(y / p.cell_size[1])
+                                : floor((y + p.wall_width) / p.cell_size[1]);
+  const double fz = p.dim == 3 ? floor(z / p.cell_size[2]) : 0.0;
+  // far outside the grid: the linear index below would overflow int
+  const double big = 1 << 20;
+  if (fabs(fx) > big || fabs(fy) > big || fabs(fz) > big) return -1;
+  int cx = (int)fx;
+  if (cx == p.Ncells[0]) cx = cx - 1;
+  int cy = (int)fy;
+  if (p.wall == 0 && cy == p.Ncells[1]) cy = cy - 1;
+  long long c;
+  if (p.dim == 3) {
+    int cz = (int)fz;
+    if (cz == p.Ncells[2]) cz = cz - 1;
+    c = (long long)cz * p.Ncells[0] * p.Ncells[1] + (long long)cy * p.Ncells[0] + cx;
+  } else {
+    c = (long long)cy * p.Ncells[0] + cx;
+  }
+  if (c < 0 || c > p.Ntotal_cells - 1) return -1;
+  return (int)c;
+}
+
+// The cell the pair kernels of the reference iterate around: unclamped floor
+// (kernel_densities.cu:52-60).  Returns false, leaving the outputs untouched, when the
+// position is not finite or so far outside the box that one periodic wrap of the
+// neighbour cells cannot bring them back into the grid; every cell index derived from a
+// true result is in range.
+__device__ __forceinline__ bool own_cell(const BoxParams& p, double x, double y, double z,
+                                         int& cx, int& cy, int& cz) {
+  const double fx = floor(x / p.cell_size[0]);
+  const double fy = p.wall == 0 ? floor(y / p.cell_size[1])
+                                : floor((y + p.wall_width) / p.cell_size[1]);
+  const double fz = p.dim == 3 ? floor(z / p.cell_size[2]) : 0.0;
+  // comparisons with NaN are false, so NaN fails every range test
+  if (!(fx >= 1.0 - p.Ncells[0] && fx <= 2.0 * p.Ncells[0] - 2.0)) return false;
+  if (p.wall == 0) {
+    if (!(fy >= 1.0 - p.Ncells[1] && fy <= 2.0 * p.Ncells[1] - 2.0)) return false;
+  } else if (!(fy >= -2.0 * p.Ncells[1] && fy <= 3.0 * p.Ncells[1])) {
+    return false;  // wall axis: out-of-grid rows are skipped, only int overflow matters
+  }
+  if (p.dim == 3 && !(fz >= 1.0 - p.Ncells[2] && fz <= 2.0 * p.Ncells[2] - 2.0)) return false;
+  cx = (int)fx;
+  cy = (int)fy;
+  cz = (int)fz;
+  return true;
+}
+
+__device__ __forceinline__ void raise_status(const Dev& d, unsigned bit, int info) {
+  unsigned old = atomicOr(d.status, bit);
+  if (!(old & bit) && bit != kStatCapacity) atomicExch(&d.err_info[0], info);
+}
+
+
+template <typename T>
+__device__ __forceinline__ void write_record(const Dev& d, int i, const BoxParams& p, int ti,
+                                             double dens, double press) {
+  using Rec = typename RecOf<T>::type;
+  Rec* rec = reinterpret_cast<Rec*>(d.rec);
+  const int Np = d.Npad;
+  const double4 x = d.pos[i];
+  const double4 v = d.vel[i];
+  Rec r;
+  r.x = x.x; r.y = x.y; r.z = x.z;
+  r.vx = v.x; r.vy = v.y; r.vz = v.z;
+  const double nkT = p.nkT;
+  double c[6];
+#pragma unroll
+  for (int q = 0; q < 6; ++q) c[q] = d.conf[q * Np + i];
+  const double dinv = 1.0 / dens;
+  if (type_of(ti) == 0) {
+    // Pi / d^2 with Pi = p I - nkT c (kernel_forces.cu:62-88)
+    const double dsq = dinv * dinv;
+    r.P[0] = (T)((press - nkT * c[0]) * dsq);
+    r.P[1] = (T)((-nkT * c[1]) * dsq);
+    r.P[2] = (T)((press - nkT * c[2]) * dsq);
+    r.P[3] = (T)((-nkT * c[3]) * dsq);
+    r.P[4] = (T)((-nkT * c[4]) * dsq);
+    r.P[5] = (T)((press - nkT * c[5]) * dsq);
+  } else {
+    // walls / colloid particles: -nkT c, completed with the fluid partner's p and d
+#pragma unroll
+    for (int q = 0; q < 6; ++q) r.P[q] = (T)(-nkT * c[q]);
+  }
+  r.invd = (T)dinv;
+  r.tinfo = ti;
+  rec[i] = r;
+}
+
+
+struct CollView {
+  const double* cs;
+  int nc;
+};
+
+// Morris ghost velocity, fluid particle i next to wall / colloid particle j
+// (kernel_forces.cu:234-318, 590-692; kernel_vel_gradients.cu:162-247, 421-525).
+template <typename T, int DIM>
+__device__ __forceinline__ void ghost_fluid_i(const BoxParams& p, const CollView& cv,
+                                              int tj, int coll0, T xi, T yi, T zi, T yj,
+                                              const T vi[3], const T r[3], const T L[3],
+                                              const T h[3], T v[3]) {
+  const T beta_max = (T)p.beta_max;
+  if (tj == 1 || tj == 2) {
+    T di, dj, Vw;
+    if (tj == 1) {
+      di = yi - (T)p.y_bottom;
+      dj = (T)p.y_bottom - yj;
+      Vw = (T)p.V_bottom;
+    } else {
+      di = (T)p.y_top - yi;
+      dj = yj - (T)p.y_top;
+      Vw = (T)p.V_top;
+    }
+    T beta = T(1) + dj / di;
+    if (beta > beta_max) beta = beta_max;
+    if (di > T(0)) {
+      v[0] = beta * (vi[0] - Vw);
+      v[1] = beta * vi[1];
+      v[2] = beta * vi[2];
+    } else {
+      v[0] = vi[0] - Vw;
+      v[1] = vi[1];
+      v[2] = vi[2];
+    }
+    return;
+  }
+  const int c = coll0 + tj - 3, nc = cv.nc;
+  T rc[3] = {xi - (T)cv.cs[CS_X * nc + c], yi - (T)cv.cs[CS_Y * nc + c],
+             DIM == 3 ? zi - (T)cv.cs[CS_Z * nc + c] : T(0)};
+  min_image<T, DIM>(rc[0], rc[1], rc[2], L, h, p.wall);
+  const T dc = DIM == 3 ? sqrt(rc[0] * rc[0] + rc[1] * rc[1] + rc[2] * rc[2])
+                        : sqrt(rc[0] * rc[0] + rc[1] * rc[1]);
+  const T R = (T)p.coll_R;
+  const T dis = dc - R;
+  const T cvel[3] = {(T)cv.cs[CS_VX * nc + c], (T)cv.cs[CS_VY * nc + c],
+                     DIM == 3 ? (T)cv.cs[CS_VZ * nc + c] : T(0)};
+  if (dis < T(0)) {
+    v[0] = vi[0] - cvel[0];
+    v[1] = vi[1] - cvel[1];
+    v[2] = vi[2] - cvel[2];
+    return;
+  }
+  const T xs = rc[0] / dc * R, ys = rc[1] / dc * R, zs = DIM == 3 ? rc[2] / dc * R : T(0);
+  T vr[3];
+  const T wz = (T)cv.cs[CS_OZ * nc + c];
+  if (DIM == 2) {
+    vr[0] = -wz * ys;
+    vr[1] = wz * xs;
+    vr[2] = T(0);
+  } else {
+    const T wx = (T)cv.cs[CS_OX * nc + c], wy = (T)cv.cs[CS_OY * nc + c];
+    vr[0] = wy * zs - wz * ys;
+    vr[1] = wz * xs - wx * zs;
+    vr[2] = wx * ys - wy * xs;
+  }
+  const T sv0 = rc[0] / dc, sv1 = rc[1] / dc, sv2 = DIM == 3 ? rc[2] / dc : T(0);
+  const T djs = DIM == 3 ? (r[0] * sv0 + r[1] * sv1 + r[2] * sv2) - dis
+                         : (r[0] * sv0 + r[1] * sv1) - dis;
+  T beta = T(1) + djs / dis;
+  if (beta > beta_max) beta = beta_max;
+  v[0] = beta * (vi[0] - cvel[0] - vr[0]);
+  v[1] = beta * (vi[1] - cvel[1] - vr[1]);
+  v[2] = beta * (vi[2] - cvel[2] - vr[2]);
+}
+
+// Morris ghost velocity, wall / colloid particle i next to particle j
+// (kernel_forces.cu:337-418, 721-821; kernel_vel_gradients.cu:249-331, 527-630).
+template <typename T, int DIM>
+__device__ __forceinline__ void ghost_solid_i(const BoxParams& p, const CollView& cv,
+                                              int ti, int coll0, T yi, T xj, T yj, T zj,
+                                              const T vj[3], const T r[3], const T L[3],
+                                              const T h[3], T v[3]) {
+  const T beta_max = (T)p.beta_max;
+  if (ti == 1 || ti == 2) {
+    T di, dj, Vw;
+    if (ti == 1) {
+      di = (T)p.y_bottom - yi;
+      dj = yj - (T)p.y_bottom;
+      Vw = (T)p.V_bottom;
+    } else {
+      di = yi - (T)p.y_top;
+      dj = (T)p.y_top - yj;
+      Vw = (T)p.V_top;
+    }
+    T beta = T(1) + di / dj;
+    if (beta > beta_max) beta = beta_max;
+    if (dj > T(0)) {
+      v[0] = beta * (Vw - vj[0]);
+      v[1] = -beta * vj[1];
+      v[2] = -beta * vj[2];
+    } else {
+      v[0] = Vw - vj[0];
+      v[1] = -vj[1];
+      v[2] = -vj[2];
+    }
+    return;
+  }
+  const int c = coll0 + ti - 3, nc = cv.nc;
+  T rc[3] = {xj - (T)cv.cs[CS_X * nc + c], yj - (T)cv.cs[CS_Y * nc + c],
+             DIM == 3 ? zj - (T)cv.cs[CS_Z * nc + c] : T(0)};
+  min_image<T, DIM>(rc[0], rc[1], rc[2], L, h, p.wall);
+  const T dc = DIM == 3 ? sqrt(rc[0] * rc[0] + rc[1] * rc[1] + rc[2] * rc[2])
+                        : sqrt(rc[0] * rc[0] + rc[1] * rc[1]);
+  const T R = (T)p.coll_R;
+  const T djs = dc - R;
+  const T cvel[3] = {(T)cv.cs[CS_VX * nc + c], (T)cv.cs[CS_VY * nc + c],
+                     DIM == 3 ? (T)cv.cs[CS_VZ * nc + c] : T(0)};
+  if (djs < T(0)) {
+    v[0] = cvel[0] - vj[0];
+    v[1] = cvel[1] - vj[1];
+    v[2] = cvel[2] - vj[2];
+    return;
+  }
+  const T xs = rc[0] / dc * R, ys = rc[1] / dc * R, zs = DIM == 3 ? rc[2] / dc * R : T(0);
+  T vr[3];
+  const T wz = (T)cv.cs[CS_OZ * nc + c];
+  if (DIM == 2) {
+    vr[0] = -wz * ys;
+    vr[1] = wz * xs;
+    vr[2] = T(0);
+  } else {
+    const T wx = (T)cv.cs[CS_OX * nc + c], wy = (T)cv.cs[CS_OY * nc + c];
+    vr[0] = wy * zs - wz * ys;
+    vr[1] = wz * xs - wx * zs;
+    vr[2] = wx * ys - wy * xs;
+  }
+  const T sv0 = rc[0] / dc, sv1 = rc[1] / dc, sv2 = DIM == 3 ? rc[2] / dc : T(0);
+  const T dis = DIM == 3 ? (-r[0] * sv0 - r[1] * sv1 - r[2] * sv2) - djs
+                         : (-r[0] * sv0 - r[1] * sv1) - djs;
+  T beta = T(1) + dis / djs;
+  if (beta > beta_max) beta = beta_max;
+  v[0] = beta * (cvel[0] + vr[0] - vj[0]);
+  v[1] = beta * (cvel[1] + vr[1] - vj[1]);
+  v[2] = beta * (cvel[2] + vr[2] - vj[2]);
+}
+
+
+// ---------------------------------------------------------------------------------
+// Pair pass arithmetic: velocity gradient (kernel_vel_gradients.cu:15-662), forces
+// (kernel_forces.cu:15-865), external force (kernel_ext_force.cu:13-73), dc/dt
+// (kernel_dcdt.cu:15-104).  One function for one (i, j) pair, used by every pair kernel.
+// ---------------------------------------------------------------------------------
+template <typename T, int DIM>
+struct PairParams {
+  T L[3], h[3], rcutsq, rcut_inv, c_gradw, a, b;
+  __device__ __forceinline__ void load(const BoxParams& p) {
+#pragma unroll
+    for (int q = 0; q < 3; ++q) {
+      L[q] = (T)p.L[q];
+      h[q] = (T)p.halfL[q];
+    }
+    rcutsq = (T)p.rcutsq;
+    rcut_inv = (T)p.rcut_inv;
+    c_gradw = (T)p.c_gradw;
+    a = (T)p.a;
+    b = (T)p.b;
+  }
+};
+
+// the target particle i of the pass
+template <typename T, int DIM>
+struct PairOwn {
+  T x, y, z, v[3], invd, press, P[6];
+  int t;
+  bool fluid, do_grad, do_force;
+};
+
+template <typename T, int DIM>
+struct PairAcc {
+  T g[DIM][DIM];
+  T f[3];
+  __device__ __forceinline__ void zero() {
+#pragma unroll
+    for (int a = 0; a < DIM; ++a)
+#pragma unroll
+      for (int c = 0; c < DIM; ++c) g[a][c] = T(0);
+    f[0] = f[1] = f[2] = T(0);
+  }
+};
+
+template <typename T, int DIM, int MODE, typename Rec>
+__device__ __forceinline__ void load_own(const Dev& d, int i, const Rec& ri, PairOwn<T, DIM>& o) {
+  o.x = (T)ri.x;
+  o.y = (T)ri.y;
+  o.z = (T)ri.z;
+  o.v[0] = (T)ri.vx;
+  o.v[1] = (T)ri.vy;
+  o.v[2] = DIM == 3 ? (T)ri.vz : T(0);
+  o.invd = ri.invd;
+  o.press = (T)d.press[i];
+#pragma unroll
+  for (int q = 0; q < 6; ++q) o.P[q] = ri.P[q];
+  o.t = type_of(ri.tinfo);
+  o.fluid = o.t == 0;
+  // gradient: fluid particles in the fused pass, every particle in kPairGradvAll
+  o.do_grad = (MODE == kPairGradvAll) || (MODE == kPairFused && o.fluid);
+  o.do_force = MODE != kPairGradvAll;
+}
+
+template <typename T, int DIM, typename Rec>
+__device__ __forceinline__ void pair_term(const BoxParams& p, const PairParams<T, DIM>& pp,
+                                          const CollView& cv, const PairOwn<T, DIM>& o,
+                                          const Rec& rj, PairAcc<T, DIM>& acc) {
+  const int tj = type_of(rj.tinfo);
+  const bool fluid_j = tj == 0;
+  // skip rules: gradient kernel_vel_gradients.cu:126-127, forces kernel_forces.cu:157-158
+  const bool pair_grad = o.do_grad && !(o.t == tj && !o.fluid);
+  const bool pair_force = o.do_force && (o.fluid || fluid_j);
+  if (!pair_grad && !pair_force) return;
+  T r[3] = {o.x - (T)rj.x, o.y - (T)rj.y, DIM == 3 ? o.z - (T)rj.z : T(0)};
+  min_image<T, DIM>(r[0], r[1], r[2], pp.L, pp.h, p.wall);
+  const T r2 = DIM == 3 ? r[0] * r[0] + r[1] * r[1] + r[2] * r[2] : r[0] * r[0] + r[1] * r[1];
+  if (!(r2 < pp.rcutsq)) return;
+  const T vj[3] = {(T)rj.vx, (T)rj.vy, DIM == 3 ? (T)rj.vz : T(0)};
+  T v[3];
+  if (o.t == tj) {
+    v[0] = o.v[0] - vj[0];
+    v[1] = o.v[1] - vj[1];
+    v[2] = o.v[2] - vj[2];
+  } else if (o.fluid) {
+    ghost_fluid_i<T, DIM>(p, cv, tj, p.coll0, o.x, o.y, o.z, (T)rj.y, o.v, r, pp.L, pp.h, v);
+  } else {
+    ghost_solid_i<T, DIM>(p, cv, o.t, p.coll0, o.y, (T)rj.x, (T)rj.y, (T)rj.z, vj, r, pp.L,
+                          pp.h, v);
+  }
+  const T rinv = rsqrt(r2);  // r and 1/r from one reciprocal square root
+  const T rr = r2 * rinv;
+  const T gw = sph_gradw<T>(rr, pp.rcut_inv, pp.c_gradw);
+  const T e[3] = {r[0] * rinv, r[1] * rinv, DIM == 3 ? r[2] * rinv : T(0)};
+  if (pair_grad) {
+    const T s = -o.invd * gw;
+#pragma unroll
+    for (int a = 0; a < DIM; ++a) {
+      const T se = s * e[a];
+#pragma unroll
+      for (int c = 0; c < DIM; ++c) acc.g[a][c] += se * v[c];
+    }
+  }
+  if (pair_force) {
+    T Pi[6], Pj[6], di, dj;
+    if (o.fluid && fluid_j) {
+#pragma unroll
+      for (int q = 0; q < 6; ++q) {
+        Pi[q] = o.P[q];
+        Pj[q] = rj.P[q];
+      }
+      di = o.invd;
+      dj = rj.invd;
+    } else if (o.fluid) {
+      // j mirrors i's density and pressure, keeps its own c (kernel_forces.cu:217-233)
+      const T dsq = o.invd * o.invd;
+#pragma unroll
+      for (int q = 0; q < 6; ++q) {
+        Pi[q] = o.P[q];
+        const T diag = (q == 0 || q == 2 || q == 5) ? o.press : T(0);
+        Pj[q] = (diag + rj.P[q]) * dsq;
+      }
+      di = o.invd;
+      dj = o.invd;
+    } else {
+      // i takes j's density, pressure and c (kernel_forces.cu:320-336)
+#pragma unroll
+      for (int q = 0; q < 6; ++q) {
+        Pj[q] = rj.P[q];
+        Pi[q] = rj.P[q];
+      }
+      di = rj.invd;
+      dj = rj.invd;
+    }
+    const T axx = -gw * (Pi[0] + Pj[0]);
+    const T axy = -gw * (Pi[1] + Pj[1]);
+    const T ayy = -gw * (Pi[2] + Pj[2]);
+    const T aux = gw * di * dj * rinv;
+    const T aux1 = pp.a * aux;
+    if (DIM == 2) {
+      const T ev = e[0] * v[0] + e[1] * v[1];
+      acc.f[0] += axx * e[0] + axy * e[1];
+      acc.f[1] += axy * e[0] + ayy * e[1];
+      const T aux2 = pp.b * aux * ev;
+      acc.f[0] += aux1 * v[0] + aux2 * e[0];
+      acc.f[1] += aux1 * v[1] + aux2 * e[1];
+    } else {
+      const T axz = -gw * (Pi[3] + Pj[3]);
+      const T ayz = -gw * (Pi[4] + Pj[4]);
+      const T azz = -gw * (Pi[5] + Pj[5]);
+      const T ev = e[0] * v[0] + e[1] * v[1] + e[2] * v[2];
+      acc.f[0] += axx * e[0] + axy * e[1] + axz * e[2];
+      acc.f[1] += axy * e[0] + ayy * e[1] + ayz * e[2];
+      acc.f[2] += axz * e[0] + ayz * e[1] + azz * e[2];
+      const T aux2 = pp.b * aux * ev;
+      acc.f[0] += aux1 * v[0] + aux2 * e[0];
+      acc.f[1] += aux1 * v[1] + aux2 * e[1];
+      acc.f[2] += aux1 * v[2] + aux2 * e[2];
+    }
+  }
+}
+
+// stored gradient, forces with the body force, and dc/dt of particle i
+template <typename T, int DIM, int MODE, bool EXT>
+__device__ __forceinline__ void pair_store(const Dev& d, int i, const BoxParams& p,
+                                           const PairOwn<T, DIM>& o,
+                                           const PairAcc<T, DIM>& acc) {
+  const int Np2 = d.Npad;
+  if (MODE == kPairGradvAll || (MODE == kPairFused && d.gradv != nullptr && o.do_grad)) {
+    // storage order xx xy xz yx yy yz zx zy zz
+    d.gradv[0 * Np2 + i] = (double)acc.g[0][0];
+    d.gradv[1 * Np2 + i] = (double)acc.g[0][1];
+    d.gradv[3 * Np2 + i] = (double)acc.g[1][0];
+    d.gradv[4 * Np2 + i] = (double)acc.g[1][1];
+    if (DIM == 3) {
+      d.gradv[2 * Np2 + i] = (double)acc.g[0][DIM - 1];
+      d.gradv[5 * Np2 + i] = (double)acc.g[1][DIM - 1];
+      d.gradv[6 * Np2 + i] = (double)acc.g[DIM - 1][0];
+      d.gradv[7 * Np2 + i] = (double)acc.g[DIM - 1][1];
+      d.gradv[8 * Np2 + i] = (double)acc.g[DIM - 1][DIM - 1];
+    }
+  }
+  if (MODE == kPairGradvAll) return;
+  double fx = (double)acc.f[0], fy = (double)acc.f[1], fz = (double)acc.f[2];
+  if (EXT && o.fluid) {
+    const double4 xd = d.pos[i];
+    const double m = xd.w;
+    if (p.ext_force_type == 1) {
+      fx += m * p.ext_force[0];
+      fy += m * p.ext_force[1];
+      if (DIM == 3) fz += m * p.ext_force[2];
+    } else if (p.ext_force_type == 2) {
+      fx += m * p.ext_force[0] * sin(p.ky * xd.y);
+      fy += 0.0;
+      if (DIM == 3) fz += 0.0;
+    } else if (p.ext_force_type == 3) {
+      fx += (xd.y < 0.5 * p.L[1]) ? m * p.ext_force[0] : -(m * p.ext_force[0]);
+      fy += 0.0;
+      if (DIM == 3) fz += 0.0;
+    }
+  }
+  d.f[i] = fx;
+  d.f[Np2 + i] = fy;
+  if (DIM == 3) d.f[2 * Np2 + i] = fz;
+  if (MODE == kPairFused && o.fluid) {
+    // dc/dt = c.g + (c.g)^T + (I - c)/tau  (kernel_dcdt.cu:76-102)
+    const double tinv = 1.0 / p.tau;
+    const double cxx = d.conf[i], cxy = d.conf[Np2 + i], cyy = d.conf[2 * Np2 + i];
+    if (DIM == 2) {
+      const double gxx = acc.g[0][0], gxy = acc.g[0][1], gyx = acc.g[1][0], gyy = acc.g[1][1];
+      const double Axx = cxx * gxx + cxy * gyx, Axy = cxx * gxy + cxy * gyy;
+      const double Ayx = cxy * gxx + cyy * gyx, Ayy = cxy * gxy + cyy * gyy;
+      d.dcdt[i] = 2.0 * Axx + tinv * (1.0 - cxx);
+      d.dcdt[Np2 + i] = Axy + Ayx - tinv * cxy;
+      d.dcdt[2 * Np2 + i] = 2.0 * Ayy + tinv * (1.0 - cyy);
+    } else {
+      const double cxz = d.conf[3 * Np2 + i], cyz = d.conf[4 * Np2 + i], czz = d.conf[5 * Np2 + i];
+      const double gxx = acc.g[0][0], gxy = acc.g[0][1], gxz = acc.g[0][DIM - 1];
+      const double gyx = acc.g[1][0], gyy = acc.g[1][1], gyz = acc.g[1][DIM - 1];
+      const double gzx = acc.g[DIM - 1][0], gzy = acc.g[DIM - 1][1], gzz = acc.g[DIM - 1][DIM - 1];
+      const double Axx = cxx * gxx + cxy * gyx + cxz * gzx;
+      const double Axy = cxx * gxy + cxy * gyy + cxz * gzy;
+      const double Axz = cxx * gxz + cxy * gyz + cxz * gzz;
+      const double Ayx = cxy * gxx + cyy * gyx + cyz * gzx;
+      const double Ayy = cxy * gxy + cyy * gyy + cyz * gzy;
+      const double Ayz = cxy * gxz + cyy * gyz + cyz * gzz;
+      const double Azx = cxz * gxx + cyz * gyx + czz * gzx;
+      const double Azy = cxz * gxy + cyz * gyy + czz * gzy;
+      const double Azz = cxz * gxz + cyz * gyz + czz * gzz;
+      d.dcdt[i] = 2.0 * Axx + tinv * (1.0 - cxx);
+      d.dcdt[Np2 + i] = Axy + Ayx - tinv * cxy;
+      d.dcdt[2 * Np2 + i] = 2.0 * Ayy + tinv * (1.0 - cyy);
+      d.dcdt[3 * Np2 + i] = Axz + Azx - tinv * cxz;
+      d.dcdt[4 * Np2 + i] = Ayz + Azy - tinv * cyz;
+      d.dcdt[5 * Np2 + i] = 2.0 * Azz + tinv * (1.0 - czz);
+    }
+  }
+}
+
+}  // namespace sph

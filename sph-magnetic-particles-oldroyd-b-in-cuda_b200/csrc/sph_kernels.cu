@@ -12,124 +12,10 @@
 #include <math.h>
 #include <stdint.h>
 
+#include "sph_device.cuh"
 #include "sph_internal.h"
 
 namespace sph {
-
-#define SPH_FULL 0xffffffffu
-
-__device__ __forceinline__ int type_of(int t) { return t & kTypeMask; }
-__device__ __forceinline__ int box_of(int t) { return t >> kTypeBits; }
-
-template <typename T> struct V4;
-template <> struct V4<double> { using type = double4; };
-template <> struct V4<float> { using type = float4; };
-
-template <typename T> struct RecOf;
-template <> struct RecOf<double> { using type = RecD; };
-template <> struct RecOf<float> { using type = RecF; };
-
-// ---------------------------------------------------------------------------------
-// SPH kernel and its radial derivative (kernel_W.cu:13-59, kernel_gradW.cu:13-53).
-// Written branch-free: the clamped terms are exact zeros where the reference skips
-// them, so the value is the same as the branchy form.
-// ---------------------------------------------------------------------------------
-template <typename T>
-__device__ __forceinline__ T sph_w(T r, T rcut_inv, T cw) {
-  T q3 = (r * rcut_inv) * T(3);
-  T t1 = T(3) - q3, t2 = T(2) - q3, t3 = T(1) - q3;
-  T a1 = t1 * t1, a2 = t2 * t2, a3 = t3 * t3;
-  T w = (a1 * a1) * t1;
-  if (q3 < T(2)) w = w - T(6) * ((a2 * a2) * t2);
-  if (q3 < T(1)) w = w + T(15) * ((a3 * a3) * t3);
-  return cw * w;
-}
-
-template <typename T>
-__device__ __forceinline__ T sph_gradw(T r, T rcut_inv, T c_gradw) {
-  T q3 = T(3) * (r * rcut_inv);
-  T t1 = T(3) - q3, t2 = T(2) - q3, t3 = T(1) - q3;
-  T a1 = t1 * t1, a2 = t2 * t2, a3 = t3 * t3;
-  T g = a1 * a1;
-  if (q3 < T(2)) g = g - T(6) * (a2 * a2);
-  if (q3 < T(1)) g = g + T(15) * (a3 * a3);
-  return c_gradw * g;
-}
-
-// Minimum image as the reference writes it: subtract L above L/2, add L below -L/2
-// (kernel_densities.cu:90-110).  y is periodic only without walls; z only in 3D.
-template <typename T, int DIM>
-__device__ __forceinline__ void min_image(T& rx, T& ry, T& rz, const T L[3], const T h[3],
-                                          int wall) {
-  if (rx > h[0]) rx -= L[0];
-  if (rx < -h[0]) rx += L[0];
-  if (!wall) {
-    if (ry > h[1]) ry -= L[1];
-    if (ry < -h[1]) ry += L[1];
-  }
-  if (DIM == 3) {
-    if (rz > h[2]) rz -= L[2];
-    if (rz < -h[2]) rz += L[2];
-  }
-}
-
-// Cell of a position as kernel_cell_list.cu:15-63 computes it (with its clamp rules).
-// Returns the box-local linear cell, or -1 when the reference would assert
-// (kernel_cell_ranges.cu:20-23) or the position is not finite.
-__device__ __forceinline__ int hash_cell(const BoxParams& p, double x, double y, double z) {
-  if (!isfinite(x) || !isfinite(y) || (p.dim == 3 && !isfinite(z))) return -2;
-  const double fx = floor(x / p.cell_size[0]);
-  const double fy = p.wall == 0 ? floor(y / p.cell_size[1])
-                                : floor((y + p.wall_width) / p.cell_size[1]);
-  const double fz = p.dim == 3 ? floor(z / p.cell_size[2]) : 0.0;
-  // far outside the grid: the linear index below would overflow int
-  const double big = 1 << 20;
-  if (fabs(fx) > big || fabs(fy) > big || fabs(fz) > big) return -1;
-  int cx = (int)fx;
-  if (cx == p.Ncells[0]) cx = cx - 1;
-  int cy = (int)fy;
-  if (p.wall == 0 && cy == p.Ncells[1]) cy = cy - 1;
-  long long c;
-  if (p.dim == 3) {
-    int cz = (int)fz;
-    if (cz == p.Ncells[2]) cz = cz - 1;
-    c = (long long)cz * p.Ncells[0] * p.Ncells[1] + (long long)cy * p.Ncells[0] + cx;
-  } else {
-    c = (long long)cy * p.Ncells[0] + cx;
-  }
-  if (c < 0 || c > p.Ntotal_cells - 1) return -1;
-  return (int)c;
-}
-
-// The cell the pair kernels of the reference iterate around: unclamped floor
-// (kernel_densities.cu:52-60).  Returns false, leaving the outputs untouched, when the
-// position is not finite or so far outside the box that one periodic wrap of the
-// neighbour cells cannot bring them back into the grid; every cell index derived from a
-// true result is in range.
-__device__ __forceinline__ bool own_cell(const BoxParams& p, double x, double y, double z,
-                                         int& cx, int& cy, int& cz) {
-  const double fx = floor(x / p.cell_size[0]);
-  const double fy = p.wall == 0 ? floor(y / p.cell_size[1])
-                                : floor((y + p.wall_width) / p.cell_size[1]);
-  const double fz = p.dim == 3 ? floor(z / p.cell_size[2]) : 0.0;
-  // comparisons with NaN are false, so NaN fails every range test
-  if (!(fx >= 1.0 - p.Ncells[0] && fx <= 2.0 * p.Ncells[0] - 2.0)) return false;
-  if (p.wall == 0) {
-    if (!(fy >= 1.0 - p.Ncells[1] && fy <= 2.0 * p.Ncells[1] - 2.0)) return false;
-  } else if (!(fy >= -2.0 * p.Ncells[1] && fy <= 3.0 * p.Ncells[1])) {
-    return false;  // wall axis: out-of-grid rows are skipped, only int overflow matters
-  }
-  if (p.dim == 3 && !(fz >= 1.0 - p.Ncells[2] && fz <= 2.0 * p.Ncells[2] - 2.0)) return false;
-  cx = (int)fx;
-  cy = (int)fy;
-  cz = (int)fz;
-  return true;
-}
-
-__device__ __forceinline__ void raise_status(const Dev& d, unsigned bit, int info) {
-  unsigned old = atomicOr(d.status, bit);
-  if (!(old & bit) && bit != kStatCapacity) atomicExch(&d.err_info[0], info);
-}
 
 // ---------------------------------------------------------------------------------
 // Velocity Verlet, particles (kernel_move_sys_VV_part1.cu:13-114, ..._part2.cu:13-58)
@@ -425,7 +311,7 @@ __global__ void __launch_bounds__(kListWarps * 32) k_build_lists(Dev d) {
   const double oy = cy * p.cell_size[1] - (p.wall ? p.wall_width : 0.0);
   const double oz = DIM == 3 ? cz * p.cell_size[2] : 0.0;
   const float cut2 = (float)p.list_cut2;
-  const int cap = d.cap, Np = d.Npad;
+  const int cap = d.cap;
   int maxcnt = 0;
   for (int t0 = beg; t0 < end; t0 += 32) {
     const int i = t0 + lane;
@@ -615,45 +501,6 @@ __global__ void k_colloid_cells(Dev d, int nboxes) {
   }
 }
 
-// ---------------------------------------------------------------------------------
-// Density (kernel_densities.cu:16-193) over the neighbour list, with the pressure
-// (kernel_pressures.cu:13-23) and the neighbour record of the particle as epilogue.
-// ---------------------------------------------------------------------------------
-template <typename T>
-__device__ __forceinline__ void write_record(const Dev& d, int i, const BoxParams& p, int ti,
-                                             double dens, double press) {
-  using Rec = typename RecOf<T>::type;
-  Rec* rec = reinterpret_cast<Rec*>(d.rec);
-  const int Np = d.Npad;
-  const double4 x = d.pos[i];
-  const double4 v = d.vel[i];
-  Rec r;
-  r.x = x.x; r.y = x.y; r.z = x.z;
-  r.vx = v.x; r.vy = v.y; r.vz = v.z;
-  const double nkT = p.nkT;
-  double c[6];
-#pragma unroll
-  for (int q = 0; q < 6; ++q) c[q] = d.conf[q * Np + i];
-  const double dinv = 1.0 / dens;
-  if (type_of(ti) == 0) {
-    // Pi / d^2 with Pi = p I - nkT c (kernel_forces.cu:62-88)
-    const double dsq = dinv * dinv;
-    r.P[0] = (T)((press - nkT * c[0]) * dsq);
-    r.P[1] = (T)((-nkT * c[1]) * dsq);
-    r.P[2] = (T)((press - nkT * c[2]) * dsq);
-    r.P[3] = (T)((-nkT * c[3]) * dsq);
-    r.P[4] = (T)((-nkT * c[4]) * dsq);
-    r.P[5] = (T)((press - nkT * c[5]) * dsq);
-  } else {
-    // walls / colloid particles: -nkT c, completed with the fluid partner's p and d
-#pragma unroll
-    for (int q = 0; q < 6; ++q) r.P[q] = (T)(-nkT * c[q]);
-  }
-  r.invd = (T)dinv;
-  r.tinfo = ti;
-  rec[i] = r;
-}
-
 template <typename T, int DIM>
 __global__ void k_density(Dev d) {
   using V = typename V4<T>::type;
@@ -714,368 +561,115 @@ __global__ void k_pressure(Dev d) {
   write_record<T>(d, i, p, ti, dens, press);
 }
 
-// ---------------------------------------------------------------------------------
-// Pair pass: velocity gradient (kernel_vel_gradients.cu:15-662), forces
-// (kernel_forces.cu:15-865), external force (kernel_ext_force.cu:13-73) and dc/dt
-// (kernel_dcdt.cu:15-104) for each particle, from its neighbour list.
-// ---------------------------------------------------------------------------------
-struct CollView {
-  const double* cs;
-  int nc;
+// Pair pass (kernel_vel_gradients.cu:15-662 and kernel_forces.cu:15-865 in one sweep),
+// one lane per particle over its neighbour list.
+//
+// Gather: at list position k every lane needs one neighbour record (128 B in FP64, 64 B
+// in mixed precision), each at its own address.  Loaded lane by lane, one 16-byte piece
+// per instruction, that is 32 separate cache lines per instruction.  Instead the warp
+// copies the 32 records into shared memory cooperatively: kPieces consecutive lanes move
+// the pieces of one record, so one copy instruction covers whole lines of 32 / kPieces
+// records.  The copies for position k + 1 (cp.async, double buffer) are in flight while
+// position k is evaluated.  Each lane then reads its record from shared memory with
+// 16-byte loads (row stride padded by one piece: conflict-free).
+constexpr int kPairWarps = 4;
+
+template <typename Rec>
+struct PairStage {
+  static constexpr int kPieces = (int)(sizeof(Rec) / 16);  // 16-byte pieces per record
+  static constexpr int kStride = kPieces + 1;               // padded row, in pieces
+  static constexpr int kPerCopy = 32 / kPieces;             // records per copy instruction
+  union Slot {
+    int4 v[kPieces];
+    Rec r;
+  };
 };
 
-// Morris ghost velocity, fluid particle i next to wall / colloid particle j
-// (kernel_forces.cu:234-318, 590-692; kernel_vel_gradients.cu:162-247, 421-525).
-template <typename T, int DIM>
-__device__ __forceinline__ void ghost_fluid_i(const BoxParams& p, const CollView& cv,
-                                              int tj, int coll0, T xi, T yi, T zi, T yj,
-                                              const T vi[3], const T r[3], const T L[3],
-                                              const T h[3], T v[3]) {
-  const T beta_max = (T)p.beta_max;
-  if (tj == 1 || tj == 2) {
-    T di, dj, Vw;
-    if (tj == 1) {
-      di = yi - (T)p.y_bottom;
-      dj = (T)p.y_bottom - yj;
-      Vw = (T)p.V_bottom;
-    } else {
-      di = (T)p.y_top - yi;
-      dj = yj - (T)p.y_top;
-      Vw = (T)p.V_top;
-    }
-    T beta = T(1) + dj / di;
-    if (beta > beta_max) beta = beta_max;
-    if (di > T(0)) {
-      v[0] = beta * (vi[0] - Vw);
-      v[1] = beta * vi[1];
-      v[2] = beta * vi[2];
-    } else {
-      v[0] = vi[0] - Vw;
-      v[1] = vi[1];
-      v[2] = vi[2];
-    }
-    return;
-  }
-  const int c = coll0 + tj - 3, nc = cv.nc;
-  T rc[3] = {xi - (T)cv.cs[CS_X * nc + c], yi - (T)cv.cs[CS_Y * nc + c],
-             DIM == 3 ? zi - (T)cv.cs[CS_Z * nc + c] : T(0)};
-  min_image<T, DIM>(rc[0], rc[1], rc[2], L, h, p.wall);
-  const T dc = DIM == 3 ? sqrt(rc[0] * rc[0] + rc[1] * rc[1] + rc[2] * rc[2])
-                        : sqrt(rc[0] * rc[0] + rc[1] * rc[1]);
-  const T R = (T)p.coll_R;
-  const T dis = dc - R;
-  const T cvel[3] = {(T)cv.cs[CS_VX * nc + c], (T)cv.cs[CS_VY * nc + c],
-                     DIM == 3 ? (T)cv.cs[CS_VZ * nc + c] : T(0)};
-  if (dis < T(0)) {
-    v[0] = vi[0] - cvel[0];
-    v[1] = vi[1] - cvel[1];
-    v[2] = vi[2] - cvel[2];
-    return;
-  }
-  const T xs = rc[0] / dc * R, ys = rc[1] / dc * R, zs = DIM == 3 ? rc[2] / dc * R : T(0);
-  T vr[3];
-  const T wz = (T)cv.cs[CS_OZ * nc + c];
-  if (DIM == 2) {
-    vr[0] = -wz * ys;
-    vr[1] = wz * xs;
-    vr[2] = T(0);
-  } else {
-    const T wx = (T)cv.cs[CS_OX * nc + c], wy = (T)cv.cs[CS_OY * nc + c];
-    vr[0] = wy * zs - wz * ys;
-    vr[1] = wz * xs - wx * zs;
-    vr[2] = wx * ys - wy * xs;
-  }
-  const T sv0 = rc[0] / dc, sv1 = rc[1] / dc, sv2 = DIM == 3 ? rc[2] / dc : T(0);
-  const T djs = DIM == 3 ? (r[0] * sv0 + r[1] * sv1 + r[2] * sv2) - dis
-                         : (r[0] * sv0 + r[1] * sv1) - dis;
-  T beta = T(1) + djs / dis;
-  if (beta > beta_max) beta = beta_max;
-  v[0] = beta * (vi[0] - cvel[0] - vr[0]);
-  v[1] = beta * (vi[1] - cvel[1] - vr[1]);
-  v[2] = beta * (vi[2] - cvel[2] - vr[2]);
+__device__ __forceinline__ void cp_async16(void* smem, const void* gmem) {
+  const unsigned s = (unsigned)__cvta_generic_to_shared(smem);
+  asm volatile("cp.async.ca.shared.global [%0], [%1], 16;\n" ::"r"(s), "l"(gmem) : "memory");
+}
+__device__ __forceinline__ void cp_async_commit() {
+  asm volatile("cp.async.commit_group;\n" ::: "memory");
+}
+__device__ __forceinline__ void cp_async_wait_prev() {
+  asm volatile("cp.async.wait_group 1;\n" ::: "memory");
 }
 
-// Morris ghost velocity, wall / colloid particle i next to particle j
-// (kernel_forces.cu:337-418, 721-821; kernel_vel_gradients.cu:249-331, 527-630).
-template <typename T, int DIM>
-__device__ __forceinline__ void ghost_solid_i(const BoxParams& p, const CollView& cv,
-                                              int ti, int coll0, T yi, T xj, T yj, T zj,
-                                              const T vj[3], const T r[3], const T L[3],
-                                              const T h[3], T v[3]) {
-  const T beta_max = (T)p.beta_max;
-  if (ti == 1 || ti == 2) {
-    T di, dj, Vw;
-    if (ti == 1) {
-      di = (T)p.y_bottom - yi;
-      dj = yj - (T)p.y_bottom;
-      Vw = (T)p.V_bottom;
-    } else {
-      di = yi - (T)p.y_top;
-      dj = (T)p.y_top - yj;
-      Vw = (T)p.V_top;
-    }
-    T beta = T(1) + di / dj;
-    if (beta > beta_max) beta = beta_max;
-    if (dj > T(0)) {
-      v[0] = beta * (Vw - vj[0]);
-      v[1] = -beta * vj[1];
-      v[2] = -beta * vj[2];
-    } else {
-      v[0] = Vw - vj[0];
-      v[1] = -vj[1];
-      v[2] = -vj[2];
-    }
-    return;
+// Lane `lane` copies its piece of the records the warp's lanes list at one position
+// (jn: this lane's neighbour there, -1 for none) into row block `buf`.
+template <typename Rec>
+__device__ __forceinline__ void stage_records(int4* buf, const Rec* __restrict__ rec, int jn,
+                                              int lane) {
+  using St = PairStage<Rec>;
+  const int piece = lane % St::kPieces;
+#pragma unroll
+  for (int t = 0; t < St::kPieces; ++t) {
+    const int r = t * St::kPerCopy + lane / St::kPieces;
+    const int jr = __shfl_sync(SPH_FULL, jn, r);
+    if (jr >= 0)
+      cp_async16(buf + r * St::kStride + piece, reinterpret_cast<const int4*>(rec + jr) + piece);
   }
-  const int c = coll0 + ti - 3, nc = cv.nc;
-  T rc[3] = {xj - (T)cv.cs[CS_X * nc + c], yj - (T)cv.cs[CS_Y * nc + c],
-             DIM == 3 ? zj - (T)cv.cs[CS_Z * nc + c] : T(0)};
-  min_image<T, DIM>(rc[0], rc[1], rc[2], L, h, p.wall);
-  const T dc = DIM == 3 ? sqrt(rc[0] * rc[0] + rc[1] * rc[1] + rc[2] * rc[2])
-                        : sqrt(rc[0] * rc[0] + rc[1] * rc[1]);
-  const T R = (T)p.coll_R;
-  const T djs = dc - R;
-  const T cvel[3] = {(T)cv.cs[CS_VX * nc + c], (T)cv.cs[CS_VY * nc + c],
-                     DIM == 3 ? (T)cv.cs[CS_VZ * nc + c] : T(0)};
-  if (djs < T(0)) {
-    v[0] = cvel[0] - vj[0];
-    v[1] = cvel[1] - vj[1];
-    v[2] = cvel[2] - vj[2];
-    return;
-  }
-  const T xs = rc[0] / dc * R, ys = rc[1] / dc * R, zs = DIM == 3 ? rc[2] / dc * R : T(0);
-  T vr[3];
-  const T wz = (T)cv.cs[CS_OZ * nc + c];
-  if (DIM == 2) {
-    vr[0] = -wz * ys;
-    vr[1] = wz * xs;
-    vr[2] = T(0);
-  } else {
-    const T wx = (T)cv.cs[CS_OX * nc + c], wy = (T)cv.cs[CS_OY * nc + c];
-    vr[0] = wy * zs - wz * ys;
-    vr[1] = wz * xs - wx * zs;
-    vr[2] = wx * ys - wy * xs;
-  }
-  const T sv0 = rc[0] / dc, sv1 = rc[1] / dc, sv2 = DIM == 3 ? rc[2] / dc : T(0);
-  const T dis = DIM == 3 ? (-r[0] * sv0 - r[1] * sv1 - r[2] * sv2) - djs
-                         : (-r[0] * sv0 - r[1] * sv1) - djs;
-  T beta = T(1) + dis / djs;
-  if (beta > beta_max) beta = beta_max;
-  v[0] = beta * (cvel[0] + vr[0] - vj[0]);
-  v[1] = beta * (cvel[1] + vr[1] - vj[1]);
-  v[2] = beta * (cvel[2] + vr[2] - vj[2]);
 }
 
 template <typename T, int DIM, int MODE, bool EXT>
-__global__ void __launch_bounds__(128, 3) k_pairs(Dev d) {
+__global__ void __launch_bounds__(kPairWarps * 32, 3) k_pairs(Dev d) {
   using Rec = typename RecOf<T>::type;
-  const int i = blockIdx.x * blockDim.x + threadIdx.x;
-  if (i >= d.Ntot) return;
+  using St = PairStage<Rec>;
+  __shared__ int4 stage[kPairWarps][2][32 * St::kStride];
+  const int w = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const int wbase = (blockIdx.x * kPairWarps + w) * 32;
+  if (wbase >= d.Ntot) return;  // whole warps only: the lanes below cooperate
+  const int i = wbase + lane;
+  const bool active = i < d.Ntot;
+  const int is = active ? i : wbase;  // lanes past the end mirror a valid slot, compute nothing
+
   const Rec* __restrict__ rec = reinterpret_cast<const Rec*>(d.rec);
-  const int tinfo_i = d.tinfo[i];
-  const int ti = type_of(tinfo_i);
-  const BoxParams& p = d.box[box_of(tinfo_i)];
-  const T L[3] = {(T)p.L[0], (T)p.L[1], (T)p.L[2]};
-  const T h[3] = {(T)p.halfL[0], (T)p.halfL[1], (T)p.halfL[2]};
-  const T rcutsq = (T)p.rcutsq, rcut_inv = (T)p.rcut_inv, c_gradw = (T)p.c_gradw;
-  const T ca = (T)p.a, cb = (T)p.b;
+  const BoxParams& p = d.box[box_of(d.tinfo[is])];
+  PairParams<T, DIM> pp;
+  pp.load(p);
   const CollView cv{d.cs, d.ncoll};
-  const int coll0 = p.coll0;
-  const Rec ri = rec[i];
-  const T xi = (T)ri.x, yi = (T)ri.y, zi = (T)ri.z;
-  const T vi[3] = {(T)ri.vx, (T)ri.vy, DIM == 3 ? (T)ri.vz : T(0)};
-  const T invd_i = ri.invd;
-  const T press_i = (T)d.press[i];
-  T Pi0[6];
+  PairOwn<T, DIM> o;
+  load_own<T, DIM, MODE>(d, is, rec[is], o);
+  PairAcc<T, DIM> acc;
+  acc.zero();
+  const int n = active ? min(d.nbr_cnt[i], d.cap) : 0;
+  int nmax = n;
 #pragma unroll
-  for (int q = 0; q < 6; ++q) Pi0[q] = ri.P[q];
-  const bool fluid_i = ti == 0;
-  // gradient: fluid particles in the fused pass, every particle in kPairGradvAll
-  const bool do_grad = (MODE == kPairGradvAll) || (MODE == kPairFused && fluid_i);
-  const bool do_force = MODE != kPairGradvAll;
-  T g[DIM][DIM];
-#pragma unroll
-  for (int a = 0; a < DIM; ++a)
-#pragma unroll
-    for (int c = 0; c < DIM; ++c) g[a][c] = T(0);
-  T f[3] = {T(0), T(0), T(0)};
-  const int n = min(d.nbr_cnt[i], d.cap);
-  // the particle's list row, read four indices at a time one batch ahead so that the
-  // index loads overlap the arithmetic of the previous batch
-  const int4* __restrict__ row = reinterpret_cast<const int4*>(d.nbr + (size_t)i * d.cap);
-  int4 nxt = n > 0 ? __ldg(&row[0]) : make_int4(0, 0, 0, 0);
-  for (int k0 = 0; k0 < n; k0 += 4) {
-   const int4 cur = nxt;
-   if (k0 + 4 < n) nxt = __ldg(&row[(k0 >> 2) + 1]);
-   const int m = min(4, n - k0);
-#pragma unroll 1
-   for (int q = 0; q < m; ++q) {
-    const int j = q == 0 ? cur.x : q == 1 ? cur.y : q == 2 ? cur.z : cur.w;
-    if (j == i) continue;
-    const Rec rj = rec[j];
-    const int tj = type_of(rj.tinfo);
-    const bool fluid_j = tj == 0;
-    // skip rules: gradient kernel_vel_gradients.cu:126-127, forces kernel_forces.cu:157-158
-    const bool pair_grad = do_grad && !(ti == tj && !fluid_i);
-    const bool pair_force = do_force && (fluid_i || fluid_j);
-    if (!pair_grad && !pair_force) continue;
-    T r[3] = {xi - (T)rj.x, yi - (T)rj.y, DIM == 3 ? zi - (T)rj.z : T(0)};
-    min_image<T, DIM>(r[0], r[1], r[2], L, h, p.wall);
-    const T r2 = DIM == 3 ? r[0] * r[0] + r[1] * r[1] + r[2] * r[2] : r[0] * r[0] + r[1] * r[1];
-    if (!(r2 < rcutsq)) continue;
-    const T vj[3] = {(T)rj.vx, (T)rj.vy, DIM == 3 ? (T)rj.vz : T(0)};
-    T v[3];
-    if (ti == tj) {
-      v[0] = vi[0] - vj[0];
-      v[1] = vi[1] - vj[1];
-      v[2] = vi[2] - vj[2];
-    } else if (fluid_i) {
-      ghost_fluid_i<T, DIM>(p, cv, tj, coll0, xi, yi, zi, (T)rj.y, vi, r, L, h, v);
-    } else {
-      ghost_solid_i<T, DIM>(p, cv, ti, coll0, yi, (T)rj.x, (T)rj.y, (T)rj.z, vj, r, L, h, v);
+  for (int s = 16; s > 0; s >>= 1) nmax = max(nmax, __shfl_xor_sync(SPH_FULL, nmax, s));
+
+  // list row, read four indices at a time: `cur` holds the batch of the position being
+  // staged, `nxt` the following one (loaded four positions ahead)
+  const int4* __restrict__ row = reinterpret_cast<const int4*>(d.nbr + (size_t)is * d.cap);
+  int4 cur = n > 0 ? __ldg(&row[0]) : make_int4(-1, -1, -1, -1);
+  int4 nxt = n > 4 ? __ldg(&row[1]) : make_int4(-1, -1, -1, -1);
+  int4* sb = &stage[w][0][0];
+  int jc = n > 0 ? cur.x : -1;
+  stage_records<Rec>(sb, rec, jc, lane);
+  cp_async_commit();
+  for (int k = 0; k < nmax; ++k) {
+    const int k1 = k + 1;
+    if ((k1 & 3) == 0) {
+      cur = nxt;
+      if (k1 + 4 < n) nxt = __ldg(&row[(k1 >> 2) + 1]);
     }
-    const T rinv = rsqrt(r2);  // r and 1/r from one reciprocal square root
-    const T rr = r2 * rinv;
-    const T gw = sph_gradw<T>(rr, rcut_inv, c_gradw);
-    const T e[3] = {r[0] * rinv, r[1] * rinv, DIM == 3 ? r[2] * rinv : T(0)};
-    if (pair_grad) {
-      const T s = -invd_i * gw;
+    const int q = k1 & 3;
+    const int jn = k1 < n ? (q == 0 ? cur.x : q == 1 ? cur.y : q == 2 ? cur.z : cur.w) : -1;
+    if (k1 < nmax) stage_records<Rec>(sb + (k1 & 1) * 32 * St::kStride, rec, jn, lane);
+    cp_async_commit();
+    cp_async_wait_prev();  // position k has landed (this lane's copies) ...
+    __syncwarp();          // ... and every other lane's
+    if (jc >= 0 && jc != i) {
+      typename St::Slot rj;
+      const int4* src = sb + (k & 1) * 32 * St::kStride + lane * St::kStride;
 #pragma unroll
-      for (int a = 0; a < DIM; ++a) {
-        const T se = s * e[a];
-#pragma unroll
-        for (int c = 0; c < DIM; ++c) g[a][c] += se * v[c];
-      }
+      for (int t = 0; t < St::kPieces; ++t) rj.v[t] = src[t];
+      pair_term<T, DIM>(p, pp, cv, o, rj.r, acc);
     }
-    if (pair_force) {
-      T Pi[6], Pj[6], di, dj;
-      if (fluid_i && fluid_j) {
-#pragma unroll
-        for (int q = 0; q < 6; ++q) {
-          Pi[q] = Pi0[q];
-          Pj[q] = rj.P[q];
-        }
-        di = invd_i;
-        dj = rj.invd;
-      } else if (fluid_i) {
-        // j mirrors i's density and pressure, keeps its own c (kernel_forces.cu:217-233)
-        const T dsq = invd_i * invd_i;
-#pragma unroll
-        for (int q = 0; q < 6; ++q) {
-          Pi[q] = Pi0[q];
-          const T diag = (q == 0 || q == 2 || q == 5) ? press_i : T(0);
-          Pj[q] = (diag + rj.P[q]) * dsq;
-        }
-        di = invd_i;
-        dj = invd_i;
-      } else {
-        // i takes j's density, pressure and c (kernel_forces.cu:320-336)
-#pragma unroll
-        for (int q = 0; q < 6; ++q) {
-          Pj[q] = rj.P[q];
-          Pi[q] = rj.P[q];
-        }
-        di = rj.invd;
-        dj = rj.invd;
-      }
-      const T axx = -gw * (Pi[0] + Pj[0]);
-      const T axy = -gw * (Pi[1] + Pj[1]);
-      const T ayy = -gw * (Pi[2] + Pj[2]);
-      const T aux = gw * di * dj * rinv;
-      const T aux1 = ca * aux;
-      if (DIM == 2) {
-        const T ev = e[0] * v[0] + e[1] * v[1];
-        f[0] += axx * e[0] + axy * e[1];
-        f[1] += axy * e[0] + ayy * e[1];
-        const T aux2 = cb * aux * ev;
-        f[0] += aux1 * v[0] + aux2 * e[0];
-        f[1] += aux1 * v[1] + aux2 * e[1];
-      } else {
-        const T axz = -gw * (Pi[3] + Pj[3]);
-        const T ayz = -gw * (Pi[4] + Pj[4]);
-        const T azz = -gw * (Pi[5] + Pj[5]);
-        const T ev = e[0] * v[0] + e[1] * v[1] + e[2] * v[2];
-        f[0] += axx * e[0] + axy * e[1] + axz * e[2];
-        f[1] += axy * e[0] + ayy * e[1] + ayz * e[2];
-        f[2] += axz * e[0] + ayz * e[1] + azz * e[2];
-        const T aux2 = cb * aux * ev;
-        f[0] += aux1 * v[0] + aux2 * e[0];
-        f[1] += aux1 * v[1] + aux2 * e[1];
-        f[2] += aux1 * v[2] + aux2 * e[2];
-      }
-    }
+    __syncwarp();  // buffer k & 1 is refilled at position k + 2
+    jc = jn;
   }
-  }
-  const int Np2 = d.Npad;
-  if (MODE == kPairGradvAll || (MODE == kPairFused && d.gradv != nullptr && do_grad)) {
-    // storage order xx xy xz yx yy yz zx zy zz
-    d.gradv[0 * Np2 + i] = (double)g[0][0];
-    d.gradv[1 * Np2 + i] = (double)g[0][1];
-    d.gradv[3 * Np2 + i] = (double)g[1][0];
-    d.gradv[4 * Np2 + i] = (double)g[1][1];
-    if (DIM == 3) {
-      d.gradv[2 * Np2 + i] = (double)g[0][2];
-      d.gradv[5 * Np2 + i] = (double)g[1][2];
-      d.gradv[6 * Np2 + i] = (double)g[2][0];
-      d.gradv[7 * Np2 + i] = (double)g[2][1];
-      d.gradv[8 * Np2 + i] = (double)g[2][2];
-    }
-  }
-  if (MODE == kPairGradvAll) return;
-  double fx = (double)f[0], fy = (double)f[1], fz = (double)f[2];
-  if (EXT && fluid_i) {
-    const double4 xd = d.pos[i];
-    const double m = xd.w;
-    if (p.ext_force_type == 1) {
-      fx += m * p.ext_force[0];
-      fy += m * p.ext_force[1];
-      if (DIM == 3) fz += m * p.ext_force[2];
-    } else if (p.ext_force_type == 2) {
-      fx += m * p.ext_force[0] * sin(p.ky * xd.y);
-      fy += 0.0;
-      if (DIM == 3) fz += 0.0;
-    } else if (p.ext_force_type == 3) {
-      fx += (xd.y < 0.5 * p.L[1]) ? m * p.ext_force[0] : -(m * p.ext_force[0]);
-      fy += 0.0;
-      if (DIM == 3) fz += 0.0;
-    }
-  }
-  d.f[i] = fx;
-  d.f[Np2 + i] = fy;
-  if (DIM == 3) d.f[2 * Np2 + i] = fz;
-  if (MODE == kPairFused && fluid_i) {
-    // dc/dt = c.g + (c.g)^T + (I - c)/tau  (kernel_dcdt.cu:76-102)
-    const double tinv = 1.0 / p.tau;
-    const double cxx = d.conf[i], cxy = d.conf[Np2 + i], cyy = d.conf[2 * Np2 + i];
-    if (DIM == 2) {
-      const double gxx = g[0][0], gxy = g[0][1], gyx = g[1][0], gyy = g[1][1];
-      const double Axx = cxx * gxx + cxy * gyx, Axy = cxx * gxy + cxy * gyy;
-      const double Ayx = cxy * gxx + cyy * gyx, Ayy = cxy * gxy + cyy * gyy;
-      d.dcdt[i] = 2.0 * Axx + tinv * (1.0 - cxx);
-      d.dcdt[Np2 + i] = Axy + Ayx - tinv * cxy;
-      d.dcdt[2 * Np2 + i] = 2.0 * Ayy + tinv * (1.0 - cyy);
-    } else {
-      const double cxz = d.conf[3 * Np2 + i], cyz = d.conf[4 * Np2 + i], czz = d.conf[5 * Np2 + i];
-      const double gxx = g[0][0], gxy = g[0][1], gxz = g[0][DIM - 1];
-      const double gyx = g[1][0], gyy = g[1][1], gyz = g[1][DIM - 1];
-      const double gzx = g[DIM - 1][0], gzy = g[DIM - 1][1], gzz = g[DIM - 1][DIM - 1];
-      const double Axx = cxx * gxx + cxy * gyx + cxz * gzx;
-      const double Axy = cxx * gxy + cxy * gyy + cxz * gzy;
-      const double Axz = cxx * gxz + cxy * gyz + cxz * gzz;
-      const double Ayx = cxy * gxx + cyy * gyx + cyz * gzx;
-      const double Ayy = cxy * gxy + cyy * gyy + cyz * gzy;
-      const double Ayz = cxy * gxz + cyy * gyz + cyz * gzz;
-      const double Azx = cxz * gxx + cyz * gyx + czz * gzx;
-      const double Azy = cxz * gxy + cyz * gyy + czz * gzy;
-      const double Azz = cxz * gxz + cyz * gyz + czz * gzz;
-      d.dcdt[i] = 2.0 * Axx + tinv * (1.0 - cxx);
-      d.dcdt[Np2 + i] = Axy + Ayx - tinv * cxy;
-      d.dcdt[2 * Np2 + i] = 2.0 * Ayy + tinv * (1.0 - cyy);
-      d.dcdt[3 * Np2 + i] = Axz + Azx - tinv * cxz;
-      d.dcdt[4 * Np2 + i] = Ayz + Azy - tinv * cyz;
-      d.dcdt[5 * Np2 + i] = 2.0 * Azz + tinv * (1.0 - czz);
-    }
-  }
+  if (active) pair_store<T, DIM, MODE, EXT>(d, i, p, o, acc);
 }
 
 // kernel_ext_force.cu:13-73 as a separate pass (class_system::calculate_external_forces)
@@ -1517,6 +1111,7 @@ int launch_colloid_cells_n(const Launch& L, int nboxes, int max_coll) {
 }
 
 int launch_density_dim(const Launch& L, int dim) {
+  if (L.d.Ntot == 0) return 0;
   const int nb = blocks(L.d.Ntot, kT);
   if (L.prec == SPH_PREC_FP64) {
     if (dim == 3) k_density<double, 3><<<nb, kT, 0, S(L)>>>(L.d);
@@ -1539,18 +1134,20 @@ int launch_pressure(const Launch& L) {
 
 template <typename T, int DIM>
 static void pairs_dispatch(const Launch& L, int mode, int with_ext, int nb) {
+  constexpr int nt = kPairWarps * 32;
   if (mode == kPairGradvAll)
-    k_pairs<T, DIM, kPairGradvAll, false><<<nb, 128, 0, S(L)>>>(L.d);
+    k_pairs<T, DIM, kPairGradvAll, false><<<nb, nt, 0, S(L)>>>(L.d);
   else if (mode == kPairForcesOnly)
-    k_pairs<T, DIM, kPairForcesOnly, false><<<nb, 128, 0, S(L)>>>(L.d);
+    k_pairs<T, DIM, kPairForcesOnly, false><<<nb, nt, 0, S(L)>>>(L.d);
   else if (with_ext)
-    k_pairs<T, DIM, kPairFused, true><<<nb, 128, 0, S(L)>>>(L.d);
+    k_pairs<T, DIM, kPairFused, true><<<nb, nt, 0, S(L)>>>(L.d);
   else
-    k_pairs<T, DIM, kPairFused, false><<<nb, 128, 0, S(L)>>>(L.d);
+    k_pairs<T, DIM, kPairFused, false><<<nb, nt, 0, S(L)>>>(L.d);
 }
 
 int launch_pairs_dim(const Launch& L, int dim, int mode, int with_ext) {
-  const int nb = blocks(L.d.Ntot, 128);
+  if (L.d.Ntot == 0) return 0;
+  const int nb = blocks(L.d.Ntot, kPairWarps * 32);
   if (L.prec == SPH_PREC_FP64) {
     if (dim == 3) pairs_dispatch<double, 3>(L, mode, with_ext, nb);
     else pairs_dispatch<double, 2>(L, mode, with_ext, nb);
