@@ -90,6 +90,12 @@ typedef struct sph_info {
       Nlist_colloids, Ncells_colloids[3], Ntotal_cells_colloids, step, nboxes, precision;
   double rcut, rcutsq, cw, c_gradw, csq, rho0, a, b, nkT, tau, dt, cell_size[3], wall_width,
       y_bottom, y_top, V_bottom, V_top, coll_R, coll_mass, coll_I, L[3], t0, omega_magnet;
+  /* the remaining class_system scalars (src/class_system.h:13-143) */
+  int Nmax, ext_force_type;
+  double rcut_inv, c, rho, P0, ky, beta_max, ext_force[3], coll_rho, coll_rep_cuton,
+      coll_rep_cutoff, rcuton_coll_rep, rcutoff_coll_rep, rcuton_coll_rep_sq,
+      rcutoff_coll_rep_sq, rcutoff_coll, rcutoff_coll_sq, F0_rep, tau_rep, r0_magnet,
+      r0_magnet_sq, F0_magnet, cell_colloids_size[3];
 } sph_info;
 
 /* Per-particle double fields readable / writable in original particle order. */
@@ -222,10 +228,12 @@ sph_status sph_read_wall_forces(sph_ctx* ctx, double* host_out);
 
 /* Cell arrays with the reference's semantics (kernel_cell_list.cu, kernel_cell_ranges.cu):
    particle_cell / particle_index sorted by (cell, id); cell_start / cell_end written for
-   occupied cells only and otherwise keeping the values of earlier searches.  Box 0. */
+   occupied cells only and otherwise keeping the values of earlier searches.  Box 0.
+   The destinations may be host or device memory (NULL skips an array). */
 sph_status sph_export_cells(sph_ctx* ctx, int* particle_cell, int* particle_index,
                             int* cell_start, int* cell_end);
-/* Colloid coarse-grid arrays (kernel_cell_colloids_*.cu), box 0. */
+/* Colloid coarse-grid arrays (kernel_cell_colloids_*.cu), box 0; host or device
+   destinations. */
 sph_status sph_export_colloid_cells(sph_ctx* ctx, int* coll_cell, int* coll_index,
                                     int* coll_cell_start, int* coll_cell_end);
 

@@ -11,6 +11,7 @@
 #include <vector>
 
 #include "sph_internal.h"
+#include "sph_io.h"
 
 using namespace sph;
 
@@ -580,54 +581,31 @@ sph_status sph_create(const sph_input* in, const char* particles_path, const sph
 void sph_destroy(sph_ctx* ctx) {
   if (!ctx) return;
   cudaSetDevice(ctx->device);
+  // A caller may reset the device before releasing the context (the reference's driver
+  // calls cudaDeviceReset before class_system::destructor, main.cu:549-552); the reset
+  // already released the device memory, stream, events and graphs, whose handles must not
+  // be used again.  The context is alive iff its allocations are still known.
+  bool alive = false;
+  if (!ctx->allocs.empty()) {
+    cudaPointerAttributes a;
+    alive = cudaPointerGetAttributes(&a, ctx->allocs.front()) == cudaSuccess &&
+            a.type == cudaMemoryTypeDevice;
+    cudaGetLastError();
+  }
+  if (!alive) {
+    delete ctx;
+    return;
+  }
   cudaStreamSynchronize(ctx->stream);
   free_ctx(ctx);
 }
 
 sph_status sph_get_info(const sph_ctx* c, int box, sph_info* o) {
   if (!c || !o || box < 0 || box >= c->nboxes) return SPH_ERR_STATE;
-  const HostBox& hb = c->boxes[box];
-  const BoxParams& p = hb.p;
-  std::memset(o, 0, sizeof(*o));
-  o->N = p.N;
-  o->dim = p.dim;
-  o->wall = p.wall;
-  for (int q = 0; q < 3; ++q) {
-    o->Ncells[q] = p.Ncells[q];
-    o->Ncells_colloids[q] = p.Ncells_colloids[q];
-    o->cell_size[q] = p.cell_size[q];
-    o->L[q] = p.L[q];
-  }
-  o->Ntotal_cells = p.Ntotal_cells;
-  o->Nwalls = p.wall ? 2 : 0;
-  o->Nlist_walls = (int)hb.walls_list.size();
-  o->N_colloids = p.N_colloids;
-  o->Nlist_colloids = (int)hb.colloids_list.size();
-  o->Ntotal_cells_colloids = p.Ntotal_cells_colloids;
+  fill_info(c->boxes[box], o);
   o->step = (int)c->host_step;
   o->nboxes = c->nboxes;
   o->precision = c->prec;
-  o->rcut = p.rcut;
-  o->rcutsq = p.rcutsq;
-  o->cw = p.cw;
-  o->c_gradw = p.c_gradw;
-  o->csq = p.csq;
-  o->rho0 = p.rho0;
-  o->a = p.a;
-  o->b = p.b;
-  o->nkT = p.nkT;
-  o->tau = p.tau;
-  o->dt = p.dt;
-  o->wall_width = p.wall_width;
-  o->y_bottom = p.y_bottom;
-  o->y_top = p.y_top;
-  o->V_bottom = p.V_bottom;
-  o->V_top = p.V_top;
-  o->coll_R = p.coll_R;
-  o->coll_mass = p.coll_mass;
-  o->coll_I = p.coll_I;
-  o->t0 = p.t0;
-  o->omega_magnet = p.omega_magnet;
   return SPH_OK;
 }
 
@@ -951,7 +929,7 @@ sph_status sph_export_cells(sph_ctx* c, int* particle_cell, int* particle_index,
   cudaStream_t st = c->stream;
   bool ok = true;
   auto dn = [&](void* dst, const void* src, size_t bytes) {
-    if (dst && cudaMemcpyAsync(dst, src, bytes, cudaMemcpyDeviceToHost, st) != cudaSuccess) ok = false;
+    if (dst && cudaMemcpyAsync(dst, src, bytes, cudaMemcpyDefault, st) != cudaSuccess) ok = false;
   };
   dn(particle_cell, c->d.keys + p.slot0, (size_t)p.N * sizeof(int));
   dn(particle_index, c->d.vals + p.slot0, (size_t)p.N * sizeof(int));
@@ -969,7 +947,7 @@ sph_status sph_export_colloid_cells(sph_ctx* c, int* coll_cell, int* coll_index,
   cudaStream_t st = c->stream;
   bool ok = true;
   auto dn = [&](void* dst, const void* src, size_t bytes) {
-    if (dst && cudaMemcpyAsync(dst, src, bytes, cudaMemcpyDeviceToHost, st) != cudaSuccess) ok = false;
+    if (dst && cudaMemcpyAsync(dst, src, bytes, cudaMemcpyDefault, st) != cudaSuccess) ok = false;
   };
   dn(coll_cell, c->d.ccell + p.coll0, (size_t)p.N_colloids * sizeof(int));
   dn(coll_index, c->d.cindex + p.coll0, (size_t)p.N_colloids * sizeof(int));
@@ -987,6 +965,112 @@ sph_status sph_kinetic_energy(sph_ctx* c, double* host_out) {
                       cudaMemcpyDeviceToHost, c->stream) != cudaSuccess ||
       cudaStreamSynchronize(c->stream) != cudaSuccess)
     return cuda_fail(c, "kinetic_energy copy");
+  return SPH_OK;
+}
+
+// ---- binary checkpoint ----
+// Layout: 8-byte magic, then int32 version, dim, nboxes, nfields, initial_done; int64
+// Ntot, ncoll, step; then nfields particle fields (Ntot doubles each, sph_field order
+// SPH_X .. SPH_DCDT_ZZ), the particle types (Ntot int32) and the colloid state
+// (SPH_NUM_COLLOID_FIELDS x ncoll doubles).  All in original particle order.
+namespace {
+const char kCkptMagic[8] = {'S', 'P', 'H', 'C', 'K', 'P', 'T', '1'};
+constexpr int kCkptVersion = 1;
+constexpr int kCkptFields = SPH_DCDT_ZZ + 1;  // f and dc/dt: the next half-kick needs them
+struct CkptHeader {
+  char magic[8];
+  int32_t version, dim, nboxes, nfields, initial_done, pad;
+  int64_t Ntot, ncoll, step;
+};
+}  // namespace
+
+sph_status sph_save_checkpoint(sph_ctx* c, const char* path) {
+  CTX_GUARD(c);
+  if (!path) return SPH_ERR_STATE;
+  if (c->in_step) return fail(c, SPH_ERR_STATE, "checkpoint inside a half-finished step");
+  sph_status s = sph_synchronize(c);
+  if (s != SPH_OK) return s;
+  CkptHeader h;
+  std::memset(&h, 0, sizeof(h));
+  std::memcpy(h.magic, kCkptMagic, sizeof(h.magic));
+  h.version = kCkptVersion;
+  h.dim = c->dim;
+  h.nboxes = c->nboxes;
+  h.nfields = kCkptFields;
+  h.initial_done = c->initial_done ? 1 : 0;
+  h.Ntot = c->d.Ntot;
+  h.ncoll = c->d.ncoll;
+  h.step = c->host_step;
+  FILE* f = std::fopen(path, "wb");
+  if (!f) return fail(c, SPH_ERR_IO, "cannot open the checkpoint file");
+  bool ok = std::fwrite(&h, sizeof(h), 1, f) == 1;
+  std::vector<double> buf((size_t)std::max(c->d.Ntot, 1));
+  for (int k = 0; k < kCkptFields && ok; ++k) {
+    s = sph_read_field(c, k, buf.data());
+    ok = s == SPH_OK && std::fwrite(buf.data(), sizeof(double), c->d.Ntot, f) == (size_t)c->d.Ntot;
+  }
+  std::vector<int> type((size_t)std::max(c->d.Ntot, 1));
+  if (ok) {
+    s = sph_read_type(c, type.data());
+    ok = s == SPH_OK && std::fwrite(type.data(), sizeof(int), c->d.Ntot, f) == (size_t)c->d.Ntot;
+  }
+  std::vector<double> cs((size_t)kCollFields * c->d.ncoll);
+  if (ok && c->d.ncoll > 0) {
+    ok = cudaMemcpy(cs.data(), c->d.cs, cs.size() * sizeof(double), cudaMemcpyDeviceToHost) ==
+             cudaSuccess &&
+         std::fwrite(cs.data(), sizeof(double), cs.size(), f) == cs.size();
+  }
+  ok = (std::fclose(f) == 0) && ok;
+  if (!ok) return s != SPH_OK ? s : fail(c, SPH_ERR_IO, "cannot write the checkpoint");
+  return SPH_OK;
+}
+
+sph_status sph_load_checkpoint(sph_ctx* c, const char* path) {
+  CTX_GUARD(c);
+  if (!path) return SPH_ERR_STATE;
+  if (c->in_step) return fail(c, SPH_ERR_STATE, "checkpoint inside a half-finished step");
+  FILE* f = std::fopen(path, "rb");
+  if (!f) return fail(c, SPH_ERR_IO, "cannot open the checkpoint file");
+  CkptHeader h;
+  bool ok = std::fread(&h, sizeof(h), 1, f) == 1;
+  if (!ok || std::memcmp(h.magic, kCkptMagic, sizeof(h.magic)) != 0 ||
+      h.version != kCkptVersion || h.nfields != kCkptFields) {
+    std::fclose(f);
+    return fail(c, SPH_ERR_BAD_INPUT, "not a checkpoint of this format");
+  }
+  if (h.dim != c->dim || h.nboxes != c->nboxes || h.Ntot != c->d.Ntot ||
+      h.ncoll != c->d.ncoll) {
+    std::fclose(f);
+    return fail(c, SPH_ERR_BAD_INPUT, "the checkpoint belongs to a different system");
+  }
+  const size_t n = (size_t)c->d.Ntot;
+  std::vector<std::vector<double>> fields(kCkptFields, std::vector<double>(n));
+  for (int k = 0; k < kCkptFields && ok; ++k)
+    ok = std::fread(fields[k].data(), sizeof(double), n, f) == n;
+  std::vector<int> type(n), mine(n);
+  if (ok) ok = std::fread(type.data(), sizeof(int), n, f) == n;
+  std::vector<double> cs((size_t)kCollFields * c->d.ncoll);
+  if (ok && !cs.empty()) ok = std::fread(cs.data(), sizeof(double), cs.size(), f) == cs.size();
+  std::fclose(f);
+  if (!ok) return fail(c, SPH_ERR_IO, "truncated checkpoint");
+  sph_status s = sph_read_type(c, mine.data());
+  if (s != SPH_OK) return s;
+  if (type != mine) return fail(c, SPH_ERR_BAD_INPUT, "particle types differ from the checkpoint");
+  for (int k = 0; k < kCkptFields; ++k) {
+    s = sph_write_field(c, k, fields[k].data());
+    if (s != SPH_OK) return s;
+  }
+  const long long step = h.step;
+  if ((!cs.empty() && cudaMemcpy(c->d.cs, cs.data(), cs.size() * sizeof(double),
+                                 cudaMemcpyHostToDevice) != cudaSuccess) ||
+      cudaMemcpy(c->d.step, &step, sizeof(step), cudaMemcpyHostToDevice) != cudaSuccess)
+    return cuda_fail(c, "checkpoint upload");
+  c->host_step = step;
+  c->initial_done = h.initial_done != 0;
+  c->forces_live = c->initial_done;
+  c->gradv_valid = false;
+  c->pos_dirty = true;
+  drop_graphs(c);
   return SPH_OK;
 }
 

@@ -67,7 +67,11 @@ struct HostBox {
   std::vector<int> colloids_list, colloids_start;
   std::vector<double> x_center, y_center, z_center;
   std::vector<double> coll_x, coll_y, coll_z;
+  int Nmax = 0;  // reserved particles (system_constructor.cpp:62-79)
 };
+
+// Scalar summary of a box (sph_info), step / nboxes / precision left zero.
+void fill_info(const HostBox& hb, sph_info* o);
 
 // Parses a reference `input` file.  Returns SPH_OK or SPH_ERR_BAD_INPUT / SPH_ERR_IO.
 sph_status parse_input_file(const char* path, sph_input* in, std::vector<double>* coll,

@@ -507,6 +507,7 @@ sph_status build_box(const sph_input& in_, const char* particles_path, HostBox* 
   if (in.new_sim == 0) {
     int Nmax = dim == 2 ? Nxyz[0] * Ny_ctor : Nxyz[0] * Ny_ctor * Nxyz[2];
     if (nc > 0) Nmax = (int)(Nmax * 1.01);
+    hb->Nmax = Nmax;
     st = lattice_particles(hb, Nxyz, dx, Nmax, msg);
   } else {
     st = restart_particles(hb, particles_path, msg);
@@ -514,6 +515,7 @@ sph_status build_box(const sph_input& in_, const char* particles_path, HostBox* 
   if (st != SPH_OK) return st;
   const int N = (int)hb->x.size();
   p.N = N;
+  if (in.new_sim != 0) hb->Nmax = N;
   // walls_list (system_initialize.cpp:278-300): ids of wall 1 then wall 2, ascending
   hb->walls_list.clear();
   if (in.wall) {
@@ -548,12 +550,41 @@ sph_status build_box(const sph_input& in_, const char* particles_path, HostBox* 
   return SPH_OK;
 }
 
-}  // namespace sph
-
-namespace {
-void fill_info(const sph::HostBox& hb, sph_info* o) {
-  const sph::BoxParams& p = hb.p;
+// class_system scalars after constructor + initialize (system_constructor.cpp:15-79,
+// system_initialize.cpp:47-262).  The colloid cutoffs derived from the input follow
+// system_initialize.cpp:158-166 and 207-217.
+void fill_info(const HostBox& hb, sph_info* o) {
+  const BoxParams& p = hb.p;
+  const sph_input& in = hb.in;
   std::memset(o, 0, sizeof(*o));
+  o->Nmax = hb.Nmax;
+  o->ext_force_type = p.ext_force_type;
+  o->rcut_inv = p.rcut_inv;
+  o->c = in.c;
+  o->rho = in.rho;
+  o->P0 = in.P0;
+  o->ky = p.ky;
+  o->beta_max = p.beta_max;
+  for (int q = 0; q < 3; ++q) {
+    o->ext_force[q] = p.ext_force[q];
+    o->cell_colloids_size[q] = p.cell_colloids_size[q];
+  }
+  o->coll_rho = p.coll_rho;
+  o->coll_rep_cuton = in.coll_repulsion_cuton;
+  o->coll_rep_cutoff = 5.0 * p.coll_R / p.tau_rep;
+  o->F0_rep = p.F0_rep;
+  o->tau_rep = p.tau_rep;
+  o->r0_magnet = in.cutoff_magnetic;
+  o->r0_magnet_sq = p.r0_magnet_sq;
+  o->F0_magnet = p.F0_magnet;
+  if (p.N_colloids > 0) {
+    o->rcuton_coll_rep = 2.0 * p.coll_R + o->coll_rep_cuton;
+    o->rcuton_coll_rep_sq = o->rcuton_coll_rep * o->rcuton_coll_rep;
+    o->rcutoff_coll_rep = 2.0 * p.coll_R + o->coll_rep_cutoff;
+    o->rcutoff_coll_rep_sq = o->rcutoff_coll_rep * o->rcutoff_coll_rep;
+    o->rcutoff_coll = o->rcutoff_coll_rep > o->r0_magnet ? o->rcutoff_coll_rep : o->r0_magnet;
+    o->rcutoff_coll_sq = o->rcutoff_coll * o->rcutoff_coll;
+  }
   o->N = p.N;
   o->dim = p.dim;
   o->wall = p.wall;
@@ -593,6 +624,9 @@ void fill_info(const sph::HostBox& hb, sph_info* o) {
   o->omega_magnet = p.omega_magnet;
 }
 
+}  // namespace sph
+
+namespace {
 template <typename T>
 void put(T* dst, const std::vector<T>& v) {
   if (dst && !v.empty()) std::memcpy(dst, v.data(), v.size() * sizeof(T));
@@ -610,7 +644,7 @@ extern "C" sph_status sph_host_setup(const sph_input* in, const char* particles_
     return s;
   }
   if (n_out) *n_out = hb.p.N;
-  if (info) fill_info(hb, info);
+  if (info) sph::fill_info(hb, info);
   if (!out) return SPH_OK;
   if (hb.p.N > cap || (int)hb.colloids_list.size() > cap || (int)hb.walls_list.size() > cap)
     return SPH_ERR_STATE;

@@ -50,7 +50,7 @@ EXPORTS = [
     "sph_read_field_device", "sph_read_type", "sph_read_colloid_field",
     "sph_read_wall_forces", "sph_export_cells", "sph_export_colloid_cells",
     "sph_kinetic_energy", "sph_last_step_ms", "sph_kernel_launches", "sph_host_setup",
-    "sph_profile_phases", "sph_phase_name",
+    "sph_profile_phases", "sph_phase_name", "sph_save_checkpoint", "sph_load_checkpoint",
 ]
 
 c_int, c_double, c_void_p, c_char_p = ctypes.c_int, ctypes.c_double, ctypes.c_void_p, ctypes.c_char_p
@@ -93,6 +93,15 @@ class SphInfo(ctypes.Structure):
         ("V_bottom", c_double), ("V_top", c_double), ("coll_R", c_double),
         ("coll_mass", c_double), ("coll_I", c_double), ("L", c_double * 3), ("t0", c_double),
         ("omega_magnet", c_double),
+        ("Nmax", c_int), ("ext_force_type", c_int),
+        ("rcut_inv", c_double), ("c", c_double), ("rho", c_double), ("P0", c_double),
+        ("ky", c_double), ("beta_max", c_double), ("ext_force", c_double * 3),
+        ("coll_rho", c_double), ("coll_rep_cuton", c_double), ("coll_rep_cutoff", c_double),
+        ("rcuton_coll_rep", c_double), ("rcutoff_coll_rep", c_double),
+        ("rcuton_coll_rep_sq", c_double), ("rcutoff_coll_rep_sq", c_double),
+        ("rcutoff_coll", c_double), ("rcutoff_coll_sq", c_double), ("F0_rep", c_double),
+        ("tau_rep", c_double), ("r0_magnet", c_double), ("r0_magnet_sq", c_double),
+        ("F0_magnet", c_double), ("cell_colloids_size", c_double * 3),
     ]
 
 
@@ -144,6 +153,8 @@ def lib():
         L.sph_export_cells.argtypes = [c_void_p, PI, PI, PI, PI]
         L.sph_export_colloid_cells.argtypes = [c_void_p, PI, PI, PI, PI]
         L.sph_kinetic_energy.argtypes = [c_void_p, PD]
+        L.sph_save_checkpoint.argtypes = [c_void_p, c_char_p]
+        L.sph_load_checkpoint.argtypes = [c_void_p, c_char_p]
         L.sph_last_step_ms.argtypes = [c_void_p, PD]
         L.sph_kernel_launches.argtypes = [c_void_p, ctypes.POINTER(ctypes.c_longlong)]
         _lib = L
@@ -399,3 +410,11 @@ class System:
         out = np.zeros(self.nboxes, dtype=np.float64)
         self._ok(lib().sph_kinetic_energy(self._h, out.ctypes.data_as(PD)))
         return out
+
+    def save_checkpoint(self, path):
+        """Binary checkpoint of the full state (bit-exact restart)."""
+        self._ok(lib().sph_save_checkpoint(self._h, os.fsencode(path)))
+
+    def load_checkpoint(self, path):
+        """Restore a checkpoint written by a system built from the same input."""
+        self._ok(lib().sph_load_checkpoint(self._h, os.fsencode(path)))

@@ -56,3 +56,26 @@ def test_create_fails_loudly_without_a_device(tmp_path):
     with pytest.raises(sph_b200.SphError) as e:
         sph_b200.System(path)
     assert e.value.status == "SPH_ERR_CUDA"
+
+
+def test_class_system_shim_exports_every_member_function():
+    """libsph_class_system.so defines every member function include/sph_class_system.h
+    declares (the reference's class_system interface, src/class_system.h:145-650)."""
+    shim = os.path.join(os.path.dirname(sph_b200.LIB_PATH), "libsph_class_system.so")
+    assert os.path.exists(shim), "build the engine first (make)"
+    ctypes.CDLL(shim)  # loads (and finds libsph_b200.so) without a GPU
+    text = open(os.path.join(ROOT, "include", "sph_class_system.h")).read()
+    text = re.sub(r"/\*.*?\*/", "", text, flags=re.S)
+    body = text[text.index("struct class_system {"):]
+    methods = set(re.findall(r"^\s+(?:int|void|sph_ctx\*)\s+(\w+)\(", body, flags=re.M))
+    assert {"read_input", "initialize", "neighbours_search", "calculate_forces",
+            "V_Verlet_step1", "V_Verlet_step2", "print_output", "destructor"} <= methods
+    out = subprocess.run(["nm", "-DC", "--defined-only", shim], capture_output=True, text=True,
+                         check=True).stdout
+    defined = set(re.findall(r"class_system::(\w+)\(", out))
+    assert methods <= defined, sorted(methods - defined)
+
+
+def test_drivers_are_built():
+    lib_dir = os.path.dirname(sph_b200.LIB_PATH)
+    assert os.access(os.path.join(lib_dir, "sph_run"), os.X_OK)
