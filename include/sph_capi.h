@@ -217,7 +217,8 @@ sph_status sph_synchronize(sph_ctx* ctx);
 sph_status sph_read_field(sph_ctx* ctx, int field, double* host_out);
 /* Overwrite a particle field from host memory (original order). */
 sph_status sph_write_field(sph_ctx* ctx, int field, const double* host_in);
-/* Copy a particle field into a caller-owned device buffer (original order). */
+/* Copy a particle field into a caller-owned device buffer (original order).  Asynchronous
+   on the context's stream: sph_synchronize before the buffer is read on another stream. */
 sph_status sph_read_field_device(sph_ctx* ctx, int field, double* dev_out);
 /* Particle types (0 fluid, 1 bottom wall, 2 top wall, 3+k colloid k). */
 sph_status sph_read_type(sph_ctx* ctx, int* host_out);

@@ -691,11 +691,11 @@ void class_system::print_particles(double* k_x, double* k_y, double* k_z, double
   double* h[15] = {x, y, z, vx, vy, vz, mass, dens, press,
                    cxx_tensor, cxy_tensor, cyy_tensor, cxz_tensor, cyz_tensor, czz_tensor};
   sph_status s = SPH_OK;
-  for (int q = 0; q < 15 && s == SPH_OK; ++q) {
-    // refresh the caller's buffer, then the host mirror (from the buffer when there is one)
-    s = sync_field(ctx, fields[q], k[q]);
-    if (s == SPH_OK) s = k[q] ? to_host(h[q], k[q], (size_t)N) : sph_read_field(ctx, fields[q], h[q]);
-  }
+  // refresh the caller's buffers (on the engine's stream), then the host mirrors from them
+  for (int q = 0; q < 15 && s == SPH_OK; ++q) s = sync_field(ctx, fields[q], k[q]);
+  if (s == SPH_OK) s = sph_synchronize(ctx);
+  for (int q = 0; q < 15 && s == SPH_OK; ++q)
+    s = k[q] ? to_host(h[q], k[q], (size_t)N) : sph_read_field(ctx, fields[q], h[q]);
   if (s != SPH_OK) {
     report(shim_, "print_particles", s);
     return;
@@ -789,6 +789,7 @@ void class_system::print_particles_gradv(double* k_x, double* k_y, double* k_z,
   double* kg[9] = {k_gradvxx, k_gradvxy, k_gradvxz, k_gradvyx, k_gradvyy,
                    k_gradvyz, k_gradvzx, k_gradvzy, k_gradvzz};
   sph_status s = SPH_OK;
+  // sph_read_field waits for the engine's stream, so the buffer refreshes have landed too
   for (int q = 0; q < 9 && s == SPH_OK; ++q) {
     s = sync_field(ctx, SPH_GXX + q, kg[q]);
     if (s == SPH_OK) s = sph_read_field(ctx, SPH_GXX + q, g[q].data());

@@ -510,6 +510,11 @@ __device__ __forceinline__ void pair_store(const Dev& d, int i, const BoxParams&
   d.f[i] = fx;
   d.f[Np2 + i] = fy;
   if (DIM == 3) d.f[2 * Np2 + i] = fz;
+  if (MODE == kPairFused && !o.fluid) {
+    // kernel_dcdt.cu:39 leaves dc/dt of walls and colloids at its initial zero
+#pragma unroll
+    for (int q = 0; q < 6; ++q) d.dcdt[q * Np2 + i] = 0.0;
+  }
   if (MODE == kPairFused && o.fluid) {
     // dc/dt = c.g + (c.g)^T + (I - c)/tau  (kernel_dcdt.cu:76-102)
     const double tinv = 1.0 / p.tau;
@@ -521,6 +526,10 @@ __device__ __forceinline__ void pair_store(const Dev& d, int i, const BoxParams&
       d.dcdt[i] = 2.0 * Axx + tinv * (1.0 - cxx);
       d.dcdt[Np2 + i] = Axy + Ayx - tinv * cxy;
       d.dcdt[2 * Np2 + i] = 2.0 * Ayy + tinv * (1.0 - cyy);
+      // the z components stay zero in 2D
+      d.dcdt[3 * Np2 + i] = 0.0;
+      d.dcdt[4 * Np2 + i] = 0.0;
+      d.dcdt[5 * Np2 + i] = 0.0;
     } else {
       const double cxz = d.conf[3 * Np2 + i], cyz = d.conf[4 * Np2 + i], czz = d.conf[5 * Np2 + i];
       const double gxx = acc.g[0][0], gxy = acc.g[0][1], gxz = acc.g[0][DIM - 1];

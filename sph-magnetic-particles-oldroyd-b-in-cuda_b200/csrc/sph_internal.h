@@ -127,7 +127,7 @@ struct Dev {
   double* dcdt_b;  // a force evaluation and the half-kick that consumes it
   double* gradv; // 9 x Npad: xx xy xz yx yy yz zx zy zz
   void* rec;     // RecD or RecF per slot
-  int* nbr;      // cap x Npad, column major
+  int* nbr;      // Npad rows of cap entries: row i lists the neighbours of slot i
   int* nbr_cnt;  // per slot
   int* key_by_gid;
   int* keys;     // sorted keys

@@ -285,6 +285,31 @@ __global__ void k_reorder(Dev d) {
   if (k == d.Ntot - 1 || d.keys[k + 1] != key) d.cell_end[key] = k - slot0;
 }
 
+// Density contribution of one list entry (kernel_densities.cu:52-163 with kernel_W.cu):
+// the exact distance test, then W(r) with r from one reciprocal square root; the
+// particle itself (r2 = 0) contributes W(0).
+template <typename T, int DIM>
+__device__ __forceinline__ T density_term(const typename V4<T>::type& xi,
+                                          const typename V4<T>::type& xj, const T L[3],
+                                          const T h[3], int wall, T rcutsq, T rcut_inv, T cw) {
+  T rx = xi.x - xj.x, ry = xi.y - xj.y, rz = DIM == 3 ? xi.z - xj.z : T(0);
+  min_image<T, DIM>(rx, ry, rz, L, h, wall);
+  const T r2 = DIM == 3 ? rx * rx + ry * ry + rz * rz : rx * rx + ry * ry;
+  if (!(r2 < rcutsq)) return T(0);
+  const T r = r2 > T(0) ? r2 * rsqrt(r2) : T(0);
+  return sph_w<T>(r, rcut_inv, cw);
+}
+
+// Density, pressure (kernel_pressures.cu:13-23) and the neighbour record of slot i.
+template <typename T>
+__device__ __forceinline__ void density_epilogue(const Dev& d, int i, const BoxParams& p,
+                                                 double dens) {
+  d.dens[i] = dens;
+  const double press = p.csq * (d.pos[i].w * dens - p.rho0);
+  d.press[i] = press;
+  write_record<T>(d, i, p, d.tinfo[i], dens, press);
+}
+
 // One warp per cell: the cell's particles (<= 32 per round) test the candidates of the
 // 3^d neighbour cells, staged 32 at a time in shared memory as float offsets from the
 // cell corner, and append hits to their own lists.  Candidate ranges come from the
@@ -293,6 +318,10 @@ __global__ void k_reorder(Dev d) {
 // a slightly enlarged cutoff; consumers apply the exact test.  A particle whose own
 // (unclamped) cell differs from its sort cell (x exactly at L) is listed separately
 // with its own neighbour cells.
+//
+// (Summing the density over the hits inside this kernel was measured slower than the
+// separate k_density pass: the per-lane hit loops diverge and the warp runs the FP64
+// kernel evaluation for its busiest lane.)
 constexpr int kListWarps = 8;
 
 template <int DIM>
@@ -509,8 +538,7 @@ __global__ void k_density(Dev d) {
   // positions: the double state itself, or its float copy in mixed precision
   const V* __restrict__ P = sizeof(T) == 8 ? reinterpret_cast<const V*>(d.pos)
                                            : reinterpret_cast<const V*>(d.pos_f);
-  const int ti = d.tinfo[i];
-  const BoxParams& p = d.box[box_of(ti)];
+  const BoxParams& p = d.box[box_of(d.tinfo[i])];
   const T L[3] = {(T)p.L[0], (T)p.L[1], (T)p.L[2]};
   const T h[3] = {(T)p.halfL[0], (T)p.halfL[1], (T)p.halfL[2]};
   const T rcutsq = (T)p.rcutsq;
@@ -529,23 +557,10 @@ __global__ void k_density(Dev d) {
     for (int q = 0; q < 4; ++q) {
       if (q >= m) break;
       const int j = q == 0 ? cur.x : q == 1 ? cur.y : q == 2 ? cur.z : cur.w;
-      const V xj = P[j];
-      T rx = xi.x - xj.x, ry = xi.y - xj.y, rz = DIM == 3 ? xi.z - xj.z : T(0);
-      min_image<T, DIM>(rx, ry, rz, L, h, p.wall);
-      const T r2 = DIM == 3 ? rx * rx + ry * ry + rz * rz : rx * rx + ry * ry;
-      if (r2 < rcutsq) {
-        // r = r2 / sqrt(r2) through the reciprocal square root; the particle itself
-        // (r2 = 0) contributes W(0)
-        const T r = r2 > T(0) ? r2 * rsqrt(r2) : T(0);
-        dens = dens + sph_w<T>(r, rcut_inv, cw);
-      }
+      dens = dens + density_term<T, DIM>(xi, P[j], L, h, p.wall, rcutsq, rcut_inv, cw);
     }
   }
-  const double densd = (double)dens;
-  d.dens[i] = densd;
-  const double press = p.csq * (d.pos[i].w * densd - p.rho0);
-  d.press[i] = press;
-  write_record<T>(d, i, p, ti, densd, press);
+  density_epilogue<T>(d, i, p, (double)dens);
 }
 
 // kernel_pressures.cu:13-23 (standalone, also refreshes the neighbour record)
@@ -703,9 +718,13 @@ __global__ void k_dcdt(Dev d) {
   const int i = blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= d.Ntot) return;
   const int ti = d.tinfo[i];
-  if (type_of(ti) != 0) return;
-  const BoxParams& p = d.box[box_of(ti)];
   const int Np = d.Npad;
+  if (type_of(ti) != 0) {
+    // kernel_dcdt.cu:39: walls and colloids keep their initial zero
+    for (int q = 0; q < 6; ++q) d.dcdt[q * Np + i] = 0.0;
+    return;
+  }
+  const BoxParams& p = d.box[box_of(ti)];
   const double tinv = 1.0 / p.tau;
   const double* G = d.gradv;
   const double cxx = d.conf[i], cxy = d.conf[Np + i], cyy = d.conf[2 * Np + i];
@@ -716,6 +735,9 @@ __global__ void k_dcdt(Dev d) {
     d.dcdt[i] = 2.0 * Axx + tinv * (1.0 - cxx);
     d.dcdt[Np + i] = Axy + Ayx - tinv * cxy;
     d.dcdt[2 * Np + i] = 2.0 * Ayy + tinv * (1.0 - cyy);
+    d.dcdt[3 * Np + i] = 0.0;
+    d.dcdt[4 * Np + i] = 0.0;
+    d.dcdt[5 * Np + i] = 0.0;
     return;
   }
   const double cxz = d.conf[3 * Np + i], cyz = d.conf[4 * Np + i], czz = d.conf[5 * Np + i];
