@@ -21,6 +21,13 @@ e2e   : the same metric through the reference-facing C ABI with host buffers: ev
         kinetic energy back to the host (wall-clock time).
 With N > 1 GPUs every rank advances its own replica of the box (the single box does not
 shard; replicas only): weak scaling, no collective in the data path.
+
+  python bench.py --workload ensemble512 [--gpus N] [--precision fp64|mixed]
+
+The batched workload: 512 independent 2D wall-bounded boxes (side 32..128, seeded
+parameters and colloids, sph_ensemble.py) in one context per GPU, sharded over ranks by
+particle-steps (strong scaling, no exchange); the JSON line adds the same boxes run one
+at a time (`looped_single_box`, a sample of every 16th box) and the ratio.
 """
 import argparse
 import json
@@ -298,9 +305,107 @@ def run_ours(args, world, rank, local, dist):
     return 0
 
 
+ENSEMBLE_NAME = ("ensemble512: 512 independent 2D wall-bounded Oldroyd-B boxes with rotating "
+                 "magnetic colloids, side 32..128 (sph_ensemble.draw_points seed 0)")
+
+
+def timed_single_box(sph_b200, path, precision, device, steps, warmup=3):
+    """Device time (ms) of `steps` steps of one box alone, after warm-up."""
+    s = sph_b200.System(path, precision=precision, device=device)
+    s.step(warmup)
+    s.synchronize()
+    s.step(steps)
+    s.synchronize()
+    ms, n = s.last_step_ms(), s.N
+    s.close()
+    return ms, n
+
+
+def run_ensemble(args, world, rank, local, dist):
+    """The batched workload: 512 boxes advanced together in one context per GPU (boxes
+    sharded over ranks by particle-steps, no exchange during the run), against the same
+    boxes run one at a time."""
+    import sph_b200
+    import sph_ensemble
+
+    pts = sph_ensemble.draw_points(512, seed=0)
+    specs = [sph_ensemble.box_spec(pt) for pt in pts]
+    costs = [sph_ensemble.box_cost(s, 1) for s in specs]
+    parts = sph_ensemble.shard(costs, world)
+    mine = parts[rank]
+    with tempfile.TemporaryDirectory() as wd:
+        paths, _ = sph_ensemble.write_inputs([pts[b] for b in mine], wd)
+        sysm = sph_b200.System(paths, precision=args.precision, device=local)
+        n = sysm.N
+        sysm.step(args.warmup)
+        sysm.synchronize()
+        if dist is not None:
+            dist.barrier()
+        l0 = sysm.kernel_launches()
+        with ClockSampler(local) as clk:
+            sysm.step(args.steps)
+            sysm.synchronize()
+        ms = sysm.last_step_ms()
+        launches = sysm.kernel_launches() - l0
+        if dist is not None:
+            dist.barrier()
+        ms_max = max_over_ranks(dist, ms, local)
+        n_all = sum(sph_ensemble.box_cost(s, 1) for s in specs)
+        value = n_all * args.steps / (ms_max * 1e-3)
+        # e2e: every step one observables sample of every box, read back to the host
+        e2e_steps = min(args.steps, args.e2e_steps)
+        t0 = time.perf_counter()
+        for _ in range(e2e_steps):
+            sysm.step(1)
+            sysm.observe()
+            obs, _ = sysm.observables()
+        e2e_dt = max_over_ranks(dist, time.perf_counter() - t0, local)
+        nb_mine = len(mine)
+        sysm.close()
+        looped = None
+        if world == 1 and rank == 0:
+            # the same boxes one at a time: every 16th box, extrapolated by particle-steps
+            sample = list(range(0, len(mine), 16))
+            t_ms, n_s = 0.0, 0
+            for k in sample:
+                ms_b, nb = timed_single_box(sph_b200, paths[k], args.precision, local, args.steps)
+                t_ms += ms_b
+                n_s += nb
+            looped = {"value": n_s * args.steps / (t_ms * 1e-3), "unit": UNIT,
+                      "sample": "%d of the 512 boxes (every 16th), each alone in its own "
+                                "context, %d graph-replayed steps after 3 warm-up steps, CUDA "
+                                "events" % (len(sample), args.steps)}
+    if rank != 0:
+        return 0
+    line = {
+        "metric": "particle-steps/s (batched ensemble of 512 2D boxes)", "value": value,
+        "unit": UNIT, "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
+        "ms_per_step": ms_max / args.steps, "higher_is_better": True, "scaling": "strong",
+        "vs_baseline": None,
+        "dtype": "f64" if args.precision == "fp64" else "f32 pairs / f64 state",
+        "data": "synthetic (lattice initial state, seeded parameters and colloid positions)",
+        "config": {"workload": ENSEMBLE_NAME, "boxes": 512, "particles": n_all,
+                   "precision": args.precision,
+                   "parallelism": ("%d boxes on this rank of %d (sharded by particle-steps)"
+                                   % (nb_mine, world)) if world > 1 else "one context",
+                   "timing": "CUDA events around sph_step(K), max over ranks"},
+        "e2e": {"value": n_all * e2e_steps / e2e_dt, "unit": UNIT, "h2d_bytes_per_step": 0,
+                "d2h_bytes_per_step": 512 * 4 * 8, "steps": e2e_steps},
+        "gpu_launches": launches,
+        "clocks": clk.summary(),
+    }
+    if looped:
+        line["looped_single_box"] = looped
+        line["batched_over_looped"] = value / looped["value"]
+    print(json.dumps(line))
+    return 0
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--workload", default="couette3d", choices=["couette3d", "ensemble512"],
+                    help="couette3d: the headline 128^3 box; ensemble512: the batched sweep")
     ap.add_argument("--steps", type=int, default=50)
     ap.add_argument("--warmup", type=int, default=5)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
@@ -321,6 +426,14 @@ def main():
         args.warmup = 3
     world, rank, local, dist = dist_setup(args)
     try:
+        if args.workload == "ensemble512":
+            if args.impl == "reference":
+                if rank == 0:
+                    print(json.dumps({"impl": "reference", "unavailable":
+                                      "the reference runs one box per process; its looped "
+                                      "single-box figure is the couette3d reference arm"}))
+                return 0
+            return run_ensemble(args, world, rank, local, dist)
         if args.impl == "reference":
             return run_reference(args, world, rank, dist)
         return run_ours(args, world, rank, local, dist)

@@ -242,6 +242,23 @@ sph_status sph_export_colloid_cells(sph_ctx* ctx, int* coll_cell, int* coll_inde
    order in double: nboxes values. */
 sph_status sph_kinetic_energy(sph_ctx* ctx, double* host_out);
 
+/* Time-averaged observables per box (no reference counterpart; they are the targets of
+   parameter sweeps over ensembles).  sph_observe adds one sample of every box, taken
+   from the current state (asynchronous; call it between steps):
+     SPH_OBS_WALL_STRESS  wall shear stress -fx(top wall) / (Lx Lz), Lz = 1 in 2D
+                          (the wall force of class_system::calculate_force_walls);
+     SPH_OBS_N1           first normal-stress difference <nkT (cxx - cyy)> over the fluid;
+     SPH_OBS_CHAIN_ORDER  colloid chain order <P2(e . m)> over colloid pairs closer than
+                          2.5 R: e the unit bond vector, m the current field direction,
+                          P2(c) = 2c^2 - 1 in 2D, (3c^2 - 1)/2 in 3D; 0 without such pairs;
+     SPH_OBS_KE           kinetic energy (kernel_calculate_macro_vars.cu:14-40).
+   sph_observables writes nboxes x SPH_NUM_OBS averages over the samples so far (and the
+   sample count); sph_reset_observables starts over. */
+enum { SPH_OBS_WALL_STRESS = 0, SPH_OBS_N1, SPH_OBS_CHAIN_ORDER, SPH_OBS_KE, SPH_NUM_OBS };
+sph_status sph_observe(sph_ctx* ctx);
+sph_status sph_observables(sph_ctx* ctx, double* host_out, long long* nsamples);
+sph_status sph_reset_observables(sph_ctx* ctx);
+
 /* Device time of the most recent sph_step, in milliseconds, measured with CUDA events
    on the context's stream. */
 sph_status sph_last_step_ms(sph_ctx* ctx, double* ms);

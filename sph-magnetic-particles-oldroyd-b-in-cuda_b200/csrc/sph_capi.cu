@@ -24,6 +24,9 @@ struct sph_ctx {
   int key_bits = 1;
   SortScratch sort{};
   double* ke_partial = nullptr;
+  double* obs_partial = nullptr;  // 2 per KE chunk
+  double* obs_acc = nullptr;      // nboxes x SPH_NUM_OBS running sums
+  long long obs_samples = 0;
   double* scratch = nullptr;  // Ntot doubles for field transfers
   int* iscratch = nullptr;    // Ntot ints
   std::string err;
@@ -484,6 +487,8 @@ sph_status sph_create_ensemble(int nboxes, const sph_input* inputs,
   d.nkechunks = (int)kchunk.size() - 1;
   ok = ok && dalloc(c, &d.ke_chunk, kchunk.size()) && dalloc(c, &d.ke_box_chunk, kbox.size());
   ok = ok && dalloc(c, &c->ke_partial, std::max(d.nkechunks, 1));
+  ok = ok && dalloc(c, &c->obs_partial, 2 * (size_t)std::max(d.nkechunks, 1));
+  ok = ok && dalloc(c, &c->obs_acc, (size_t)SPH_NUM_OBS * nboxes);
   if (!ok) {
     fprintf(stderr, "sph_create: device allocation failed\n");
     free_ctx(c);
@@ -965,6 +970,43 @@ sph_status sph_kinetic_energy(sph_ctx* c, double* host_out) {
                       cudaMemcpyDeviceToHost, c->stream) != cudaSuccess ||
       cudaStreamSynchronize(c->stream) != cudaSuccess)
     return cuda_fail(c, "kinetic_energy copy");
+  return SPH_OK;
+}
+
+// ---- observables ----
+sph_status sph_observe(sph_ctx* c) {
+  CTX_GUARD(c);
+  if (c->in_step) return fail(c, SPH_ERR_STATE, "observe inside a half-finished step");
+  if (!c->initial_done) {
+    sph_status s = do_initial(c);
+    if (s != SPH_OK) return s;
+  }
+  if (launch_observe(launcher(c), c->ke_partial, c->obs_partial, c->obs_acc))
+    return cuda_fail(c, "observe");
+  c->obs_samples++;
+  return SPH_OK;
+}
+
+sph_status sph_observables(sph_ctx* c, double* host_out, long long* nsamples) {
+  CTX_GUARD(c);
+  if (!host_out) return SPH_ERR_STATE;
+  const size_t n = (size_t)SPH_NUM_OBS * c->nboxes;
+  if (cudaMemcpyAsync(host_out, c->obs_acc, n * sizeof(double), cudaMemcpyDeviceToHost,
+                      c->stream) != cudaSuccess ||
+      cudaStreamSynchronize(c->stream) != cudaSuccess)
+    return cuda_fail(c, "observables");
+  const double inv = c->obs_samples > 0 ? 1.0 / (double)c->obs_samples : 0.0;
+  for (size_t k = 0; k < n; ++k) host_out[k] *= inv;
+  if (nsamples) *nsamples = c->obs_samples;
+  return SPH_OK;
+}
+
+sph_status sph_reset_observables(sph_ctx* c) {
+  CTX_GUARD(c);
+  if (cudaMemsetAsync(c->obs_acc, 0, (size_t)SPH_NUM_OBS * c->nboxes * sizeof(double),
+                      c->stream) != cudaSuccess)
+    return cuda_fail(c, "reset_observables");
+  c->obs_samples = 0;
   return SPH_OK;
 }
 

@@ -203,6 +203,8 @@ int launch_colloid_forces(const Launch& L, int with_pairs);
 int launch_advance_time(const Launch& L, int mode);
 int launch_count_step(const Launch& L);
 int launch_kinetic_energy(const Launch& L, double* partial);
+// one observables sample of every box added to acc (nboxes x 4), KE included
+int launch_observe(const Launch& L, double* ke_partial, double* obs_partial, double* acc);
 int launch_gather_field(const Launch& L, int field, double* out);
 int launch_scatter_field(const Launch& L, int field, const double* in);
 int launch_gather_int(const Launch& L, const int* src, int* out);

@@ -993,6 +993,81 @@ __global__ void k_ke_final(Dev d, const double* partial) {
   d.ke[b] = ke;
 }
 
+// ---------------------------------------------------------------------------------
+// Observables (no reference counterpart), one sample per box added to running sums:
+//  [0] wall shear stress  -fx(top wall) / (Lx Lz), Lz = 1 in 2D (0 without walls);
+//  [1] first normal-stress difference  N1 = <nkT (cxx - cyy)> over the fluid;
+//  [2] chain order  <P2(e . m)> over colloid pairs closer than 2.5 R, e the unit bond and
+//      m the current field direction; P2(c) = 2c^2 - 1 in 2D (cos 2 phi), (3c^2 - 1)/2 in
+//      3D; 0 when no pair is that close;
+//  [3] kinetic energy (k_ke_final must have run for this sample).
+// Fixed-order reductions (slot chunks that never straddle boxes, then chunks in order),
+// so the sums are bit-reproducible.
+// ---------------------------------------------------------------------------------
+__global__ void __launch_bounds__(kRedThreads) k_obs_partial(Dev d, double* partial) {
+  __shared__ double sh[2][kRedThreads];
+  const int c = blockIdx.x;
+  const int lo = d.ke_chunk[c], hi = d.ke_chunk[c + 1];
+  const int Np = d.Npad;
+  double v[2] = {0.0, 0.0};  // sum of nkT (cxx - cyy) over fluid, fluid count
+  for (int i = lo + threadIdx.x; i < hi; i += kRedThreads) {
+    const int ti = d.tinfo[i];
+    if (type_of(ti) != 0) continue;
+    v[0] += d.box[box_of(ti)].nkT * (d.conf[i] - d.conf[2 * Np + i]);
+    v[1] += 1.0;
+  }
+  block_reduce<2>(v, sh);
+  if (threadIdx.x == 0) {
+    partial[2 * c] = v[0];
+    partial[2 * c + 1] = v[1];
+  }
+}
+
+__global__ void k_obs_final(Dev d, const double* partial, double* acc) {
+  const int b = blockIdx.x * blockDim.x + threadIdx.x;
+  if (b >= d.nboxes) return;
+  const BoxParams& p = d.box[b];
+  double n1 = 0.0, nf = 0.0;
+  for (int c = d.ke_box_chunk[b]; c < d.ke_box_chunk[b + 1]; ++c) {
+    n1 += partial[2 * c];
+    nf += partial[2 * c + 1];
+  }
+  n1 = nf > 0.0 ? n1 / nf : 0.0;
+  double tw = 0.0;
+  if (p.wall) tw = -d.wall_f[3 * (p.wall_seg0 + 1)] / (p.L[0] * (p.dim == 3 ? p.L[2] : 1.0));
+  double so = 0.0;
+  int npair = 0;
+  const double mx = d.mag[3 * b], my = d.mag[3 * b + 1], mz = d.mag[3 * b + 2];
+  const double mn = sqrt(mx * mx + my * my + mz * mz);
+  const double rmax2 = (2.5 * p.coll_R) * (2.5 * p.coll_R);
+  const int nc = d.ncoll, c0 = p.coll0;
+  for (int a = 0; a < p.N_colloids && mn > 0.0; ++a)
+    for (int e = a + 1; e < p.N_colloids; ++e) {
+      double rx = d.cs[CS_X * nc + c0 + a] - d.cs[CS_X * nc + c0 + e];
+      double ry = d.cs[CS_Y * nc + c0 + a] - d.cs[CS_Y * nc + c0 + e];
+      double rz = p.dim == 3 ? d.cs[CS_Z * nc + c0 + a] - d.cs[CS_Z * nc + c0 + e] : 0.0;
+      if (rx > p.halfL[0]) rx -= p.L[0];
+      if (rx < -p.halfL[0]) rx += p.L[0];
+      if (!p.wall) {
+        if (ry > p.halfL[1]) ry -= p.L[1];
+        if (ry < -p.halfL[1]) ry += p.L[1];
+      }
+      if (p.dim == 3) {
+        if (rz > p.halfL[2]) rz -= p.L[2];
+        if (rz < -p.halfL[2]) rz += p.L[2];
+      }
+      const double r2 = rx * rx + ry * ry + rz * rz;
+      if (!(r2 < rmax2) || r2 <= 0.0) continue;
+      const double cs = (rx * mx + ry * my + rz * mz) / (sqrt(r2) * mn);
+      so += p.dim == 3 ? 1.5 * cs * cs - 0.5 : 2.0 * cs * cs - 1.0;
+      ++npair;
+    }
+  acc[4 * b + 0] += tw;
+  acc[4 * b + 1] += n1;
+  acc[4 * b + 2] += npair > 0 ? so / npair : 0.0;
+  acc[4 * b + 3] += d.ke[b];
+}
+
 // Field gather / scatter between slot order and original order.
 __device__ __forceinline__ double* field_ptr(const Dev& d, int f, int& comp, bool& in_pos,
                                              bool& in_vel) {
@@ -1221,6 +1296,14 @@ int launch_kinetic_energy(const Launch& L, double* partial) {
   k_ke_partial<<<L.d.nkechunks, kRedThreads, 0, S(L)>>>(L.d, partial);
   if (check(L)) return 1;
   k_ke_final<<<blocks(L.d.nboxes, 64), 64, 0, S(L)>>>(L.d, partial);
+  return check(L);
+}
+
+int launch_observe(const Launch& L, double* ke_partial, double* obs_partial, double* acc) {
+  if (launch_kinetic_energy(L, ke_partial)) return 1;
+  k_obs_partial<<<L.d.nkechunks, kRedThreads, 0, S(L)>>>(L.d, obs_partial);
+  if (check(L)) return 1;
+  k_obs_final<<<blocks(L.d.nboxes, 64), 64, 0, S(L)>>>(L.d, obs_partial, acc);
   return check(L);
 }
 

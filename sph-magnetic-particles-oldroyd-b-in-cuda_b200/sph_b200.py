@@ -51,7 +51,9 @@ EXPORTS = [
     "sph_read_wall_forces", "sph_export_cells", "sph_export_colloid_cells",
     "sph_kinetic_energy", "sph_last_step_ms", "sph_kernel_launches", "sph_host_setup",
     "sph_profile_phases", "sph_phase_name", "sph_save_checkpoint", "sph_load_checkpoint",
+    "sph_observe", "sph_observables", "sph_reset_observables",
 ]
+OBSERVABLES = ["wall_stress", "N1", "chain_order", "kinetic_energy"]
 
 c_int, c_double, c_void_p, c_char_p = ctypes.c_int, ctypes.c_double, ctypes.c_void_p, ctypes.c_char_p
 PD = ctypes.POINTER(ctypes.c_double)
@@ -154,6 +156,9 @@ def lib():
         L.sph_export_colloid_cells.argtypes = [c_void_p, PI, PI, PI, PI]
         L.sph_kinetic_energy.argtypes = [c_void_p, PD]
         L.sph_save_checkpoint.argtypes = [c_void_p, c_char_p]
+        L.sph_observe.argtypes = [c_void_p]
+        L.sph_observables.argtypes = [c_void_p, PD, ctypes.POINTER(ctypes.c_longlong)]
+        L.sph_reset_observables.argtypes = [c_void_p]
         L.sph_load_checkpoint.argtypes = [c_void_p, c_char_p]
         L.sph_last_step_ms.argtypes = [c_void_p, PD]
         L.sph_kernel_launches.argtypes = [c_void_p, ctypes.POINTER(ctypes.c_longlong)]
@@ -410,6 +415,20 @@ class System:
         out = np.zeros(self.nboxes, dtype=np.float64)
         self._ok(lib().sph_kinetic_energy(self._h, out.ctypes.data_as(PD)))
         return out
+
+    def observe(self):
+        """Add one sample of every box's observables (asynchronous)."""
+        self._ok(lib().sph_observe(self._h))
+
+    def observables(self):
+        """(nboxes x 4 time averages in OBSERVABLES order, number of samples)."""
+        out = np.zeros((self.nboxes, len(OBSERVABLES)), dtype=np.float64)
+        n = ctypes.c_longlong(0)
+        self._ok(lib().sph_observables(self._h, out.ctypes.data_as(PD), ctypes.byref(n)))
+        return out, n.value
+
+    def reset_observables(self):
+        self._ok(lib().sph_reset_observables(self._h))
 
     def save_checkpoint(self, path):
         """Binary checkpoint of the full state (bit-exact restart)."""
