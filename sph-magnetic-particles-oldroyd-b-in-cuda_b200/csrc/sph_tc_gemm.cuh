@@ -1,0 +1,189 @@
+// sph_tc_gemm.cuh -- BF16 tensor-core GEMM for sm_100a (tcgen05 / TMEM), used by the
+// surrogate network (sph_mlp.cu).
+//
+//   C[M x N] = A[M x K] . B[N x K]^T     A, B bf16 with K contiguous, C accumulated in FP32
+//
+// One CTA (4 warps) computes a 128 x N tile (N <= 256, a multiple of 16) for one "head"
+// (blockIdx.y selects per-head operand offsets).  K is walked in chunks of 64: all threads
+// copy the chunk of A (128 rows) and B (N rows) into shared memory in the canonical
+// K-major, no-swizzle UMMA layout (core matrices of 8 rows x 16 bytes), one elected thread
+// issues four tcgen05.mma (K = 16 each) accumulating into a 128-lane x N-column FP32 tile
+// in tensor memory, and tcgen05.commit signals an mbarrier when they have read the chunk.
+// The epilogue reads the accumulator back with tcgen05.ld (warp w owns TMEM lanes
+// 32w..32w+31, i.e. rows), and each thread finishes one row.
+//
+// Shared-memory descriptor (64 bits): start address >> 4 in [0,14), leading byte offset
+// >> 4 in [16,30) (distance between the two core matrices along K of one K = 16 step:
+// 128 B), stride byte offset >> 4 in [32,46) (distance between 8-row groups:
+// kChunkK / 8 * 128 B), version 1 in [46,48), layout SWIZZLE_NONE (0) in [61,64).
+// Instruction descriptor (kind::f16): D format F32 (bit 4), A and B format BF16 (bits 7,
+// 10), both K-major, N >> 3 in [17,23), M >> 4 in [24,29).
+#pragma once
+
+#include <cuda_bf16.h>
+#include <cstdint>
+
+namespace sph {
+namespace tc {
+
+constexpr int kTileM = 128;
+constexpr int kChunkK = 64;
+constexpr int kMaxN = 256;
+constexpr int kSbo = kChunkK / 8 * 128;  // bytes between 8-row groups
+// dynamic shared memory per CTA: A and B chunks, padded so that one CTA occupies an SM
+// (its 256 TMEM columns are then never contended)
+constexpr int kSmemBytes = 120 * 1024;
+constexpr int kTmemCols = 256;
+constexpr long long kSpinLimit = 1ll << 26;  // bounded mbarrier wait
+
+__device__ __forceinline__ uint32_t smem_u32(const void* p) {
+  return (uint32_t)__cvta_generic_to_shared(p);
+}
+
+__device__ __forceinline__ uint32_t core_offset(int row, int k8) {
+  return (uint32_t)((row >> 3) * kSbo + k8 * 128 + (row & 7) * 16);
+}
+
+__device__ __forceinline__ uint64_t smem_desc(uint32_t addr) {
+  const uint64_t lbo = 128 >> 4, sbo = kSbo >> 4;
+  return (uint64_t)((addr >> 4) & 0x3FFFu) | (lbo << 16) | (sbo << 32) | (1ull << 46);
+}
+
+__host__ __device__ constexpr uint32_t idesc_bf16_f32(int M, int N) {
+  return (1u << 4) | (1u << 7) | (1u << 10) | ((uint32_t)(N >> 3) << 17) |
+         ((uint32_t)(M >> 4) << 24);
+}
+
+__device__ __forceinline__ void fence_before_sync() {
+  asm volatile("tcgen05.fence::before_thread_sync;\n" ::: "memory");
+}
+__device__ __forceinline__ void fence_after_sync() {
+  asm volatile("tcgen05.fence::after_thread_sync;\n" ::: "memory");
+}
+
+__device__ __forceinline__ void tmem_alloc(uint32_t* dst_smem, int cols) {
+  asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;\n" ::"r"(
+                   smem_u32(dst_smem)),
+               "r"(cols)
+               : "memory");
+}
+__device__ __forceinline__ void tmem_free(uint32_t taddr, int cols) {
+  asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;\n" ::"r"(taddr), "r"(cols)
+               : "memory");
+  asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;\n" ::: "memory");
+}
+
+__device__ __forceinline__ void mbar_init(uint64_t* bar, int count) {
+  asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;\n" ::"r"(smem_u32(bar)), "r"(count)
+               : "memory");
+}
+
+// Waits for the phase `parity` of the mbarrier to complete; gives up after kSpinLimit
+// polls and returns false.
+__device__ __forceinline__ bool mbar_wait(uint64_t* bar, uint32_t parity) {
+  const uint32_t a = smem_u32(bar);
+  for (long long it = 0; it < kSpinLimit; ++it) {
+    uint32_t done;
+    asm volatile(
+        "{\n .reg .pred p;\n mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n"
+        " selp.u32 %0, 1, 0, p;\n}\n"
+        : "=r"(done)
+        : "r"(a), "r"(parity)
+        : "memory");
+    if (done) return true;
+  }
+  return false;
+}
+
+__device__ __forceinline__ void mma_bf16(uint32_t tmem_d, uint64_t da, uint64_t db, uint32_t idesc,
+                                         int accumulate) {
+  asm volatile(
+      "{\n .reg .pred p;\n setp.ne.b32 p, %4, 0;\n"
+      " tcgen05.mma.cta_group::1.kind::f16 [%0], %1, %2, %3, p;\n}\n" ::"r"(tmem_d),
+      "l"(da), "l"(db), "r"(idesc), "r"(accumulate)
+      : "memory");
+}
+
+__device__ __forceinline__ void mma_commit(uint64_t* bar) {
+  asm volatile(
+      "tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];\n" ::"r"(
+          smem_u32(bar))
+      : "memory");
+}
+
+// 16 consecutive FP32 columns of this thread's TMEM lane.
+__device__ __forceinline__ void tmem_ld16(uint32_t taddr, float (&v)[16]) {
+  uint32_t r[16];
+  asm volatile(
+      "tcgen05.ld.sync.aligned.32x32b.x16.b32 {%0,%1,%2,%3,%4,%5,%6,%7,%8,%9,%10,%11,%12,%13,"
+      "%14,%15}, [%16];\n"
+      : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]), "=r"(r[6]),
+        "=r"(r[7]), "=r"(r[8]), "=r"(r[9]), "=r"(r[10]), "=r"(r[11]), "=r"(r[12]), "=r"(r[13]),
+        "=r"(r[14]), "=r"(r[15])
+      : "r"(taddr)
+      : "memory");
+  asm volatile("tcgen05.wait::ld.sync.aligned;\n" ::: "memory");
+#pragma unroll
+  for (int q = 0; q < 16; ++q) v[q] = __uint_as_float(r[q]);
+}
+
+// Operands of one GEMM launch; head h uses A + h * strideA, B + h * strideB (elements).
+struct GemmArgs {
+  const __nv_bfloat16* A;
+  const __nv_bfloat16* B;
+  long long strideA, strideB;
+  int lda, ldb;  // row pitch (elements), multiples of 8
+  int M, N, K;   // M % 128 == 0, N % 16 == 0 and N <= 256, K % 64 == 0
+  int* err;      // set to 1 when a wait gives up
+};
+
+// Copies rows [r0, r0 + rows) x K-chunk [k0, k0 + 64) of a K-contiguous bf16 matrix into
+// the canonical layout at dst.
+__device__ __forceinline__ void load_chunk(uint8_t* dst, const __nv_bfloat16* src, int ld, int r0,
+                                           int rows, int k0) {
+  for (int idx = threadIdx.x; idx < rows * (kChunkK / 8); idx += blockDim.x) {
+    const int r = idx >> 3, k8 = idx & 7;
+    const uint4 v = *reinterpret_cast<const uint4*>(src + (size_t)(r0 + r) * ld + k0 + k8 * 8);
+    *reinterpret_cast<uint4*>(dst + core_offset(r, k8)) = v;
+  }
+}
+
+// The main loop: leaves the 128 x N FP32 accumulator of this CTA's tile in TMEM columns
+// [tmem, tmem + N).  Returns false if an MMA completion was not observed in time.
+__device__ __forceinline__ bool gemm_mainloop(const GemmArgs& g, uint8_t* smem, uint64_t* bar,
+                                              uint32_t tmem) {
+  const int head = blockIdx.y;
+  const int m0 = blockIdx.x * kTileM;
+  const __nv_bfloat16* A = g.A + head * g.strideA;
+  const __nv_bfloat16* B = g.B + head * g.strideB;
+  uint8_t* sA = smem;
+  uint8_t* sB = smem + kTileM * kChunkK * 2;
+  const uint32_t idesc = idesc_bf16_f32(kTileM, g.N);
+  uint32_t parity = 0;
+  bool ok = true;
+  for (int k0 = 0; k0 < g.K; k0 += kChunkK) {
+    load_chunk(sA, A, g.lda, m0, kTileM, k0);
+    load_chunk(sB, B, g.ldb, 0, g.N, k0);
+    // generic-proxy stores -> visible to the tensor core's (async proxy) reads
+    asm volatile("fence.proxy.async.shared::cta;\n" ::: "memory");
+    fence_before_sync();
+    __syncthreads();
+    fence_after_sync();
+    if (threadIdx.x == 0) {
+#pragma unroll
+      for (int s = 0; s < kChunkK / 16; ++s)
+        mma_bf16(tmem, smem_desc(smem_u32(sA) + s * 256), smem_desc(smem_u32(sB) + s * 256),
+                 idesc, (k0 > 0 || s > 0) ? 1 : 0);
+      mma_commit(bar);
+    }
+    // the next chunk overwrites sA / sB: wait until the MMAs have consumed them
+    ok = mbar_wait(bar, parity) && ok;
+    parity ^= 1u;
+    fence_after_sync();
+    if (!ok) break;
+  }
+  return ok;
+}
+
+}  // namespace tc
+}  // namespace sph
