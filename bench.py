@@ -28,6 +28,13 @@ The batched workload: 512 independent 2D wall-bounded boxes (side 32..128, seede
 parameters and colloids, sph_ensemble.py) in one context per GPU, sharded over ranks by
 particle-steps (strong scaling, no exchange); the JSON line adds the same boxes run one
 at a time (`looped_single_box`, a sample of every 16th box) and the ratio.
+
+  python bench.py --workload sweep [--sweep-train 20480] [--sweep-steps 2000]
+
+Sweep points per hour: 20,480 sweep points solved by the batched solver train the
+surrogate (5 heads); 65,536 query points are predicted and those on which the heads
+disagree by more than 2% are re-solved; 512 held-out points re-solved by the solver give
+the wall-stress error; one-at-a-time plain runs (a sample of 8) give the baseline rate.
 """
 import argparse
 import json
@@ -401,15 +408,112 @@ def run_ensemble(args, world, rank, local, dist):
     return 0
 
 
+SWEEP_NAME = ("sweep: 2D wall-bounded Oldroyd-B boxes with magnetic colloids at side 64, six "
+               "physical inputs sampled over the batched workload's ranges; observables "
+               "averaged over the last 75 percent of {steps} steps")
+
+
+def sweep_line(args, nsteps, ntrain, nquery, t_one, t_data, npts, t_train, t_pred, t_fallback,
+               mean_te, route_te, Yte, Ytr, route_q):
+    """The JSON line of the sweep benchmark (kept apart so that it is tested on the CPU)."""
+    import sph_surrogate
+
+    keep = ~route_te
+    err_kept = sph_surrogate.relative_error(mean_te[keep, 0], Yte[keep, 0]) if keep.any() else None
+    err_all = sph_surrogate.relative_error(mean_te[:, 0], Yte[:, 0])
+    base = sph_surrogate.relative_error(np.full(len(Yte), Ytr[:, 0].mean()), Yte[:, 0])
+
+    def per_hour(n, s):
+        return 3600.0 * n / s if s > 0 else None
+
+    sur_marginal = per_hour(nquery, t_pred + t_fallback)
+    one = per_hour(1, float(np.mean(t_one)))
+    return {
+        "metric": "sweep points/h at <=1% wall-stress error (surrogate with solver fallback)",
+        "value": sur_marginal, "unit": "points/h", "n_gpus": 1, "higher_is_better": True,
+        "scaling": "strong", "vs_baseline": None, "dtype": "bf16 network / " + args.precision,
+        "data": "synthetic (seeded sweep points)",
+        "config": {"workload": SWEEP_NAME.format(steps=nsteps), "train_points": ntrain,
+                   "heldout": len(Yte), "queries": nquery, "heads": 5,
+                   "train_steps": args.sweep_train_steps, "batch": 1024, "route_tol": 0.02},
+        "one_at_a_time_points_per_h": one,
+        "batched_points_per_h": per_hour(npts, t_data),
+        "surrogate_points_per_h_incl_data_and_training":
+            per_hour(nquery, t_data + t_train + t_pred + t_fallback),
+        "over_one_at_a_time": sur_marginal / one if sur_marginal and one else None,
+        "heldout_wall_stress_error": {"unrouted": err_kept, "all": err_all,
+                                      "mean_predictor": base, "measure": "mean |pred - true| / "
+                                      "mean |true| over held-out points re-solved by the solver"},
+        "heldout_errors_all_targets": [sph_surrogate.relative_error(mean_te[:, k], Yte[:, k])
+                                       for k in range(4)],
+        "routed_fraction": float(np.mean(route_q)),
+        "seconds": {"one_point_mean": float(np.mean(t_one)), "training_data": t_data,
+                    "training": t_train, "predict": t_pred, "fallback": t_fallback},
+        "accepted": bool(err_kept is not None and err_kept <= 0.01),
+    }
+
+
+def run_sweep_bench(args, world, rank, local, dist):
+    """Sweep points per hour: one-at-a-time plain runs, the batched solver, and the batched
+    solver plus the surrogate (routing the points where its heads disagree back to the
+    solver), with the surrogate's error on held-out points re-solved by the solver."""
+    import sph_b200
+    import sph_ensemble
+    import sph_surrogate
+
+    if world > 1 and rank != 0:
+        return 0
+    nsteps, ntrain, nquery = args.sweep_steps, args.sweep_train, 65536
+    pts = sph_ensemble.draw_points(ntrain + 512, seed=1, fixed_N=64, coll_seed=7)
+    queries = sph_ensemble.draw_points(nquery, seed=2, fixed_N=64, coll_seed=7)
+    # the plain method one point at a time (a sample, each in its own context)
+    t_one = []
+    with tempfile.TemporaryDirectory() as wd:
+        paths, _ = sph_ensemble.write_inputs(pts[:8], wd, nsteps=nsteps)
+        for p in paths:
+            t0 = time.perf_counter()
+            s = sph_b200.System(p, precision=args.precision, device=local)
+            sph_ensemble.run_sweep(s, nsteps, 20, warm=nsteps // 4)
+            s.close()
+            t_one.append(time.perf_counter() - t0)
+    # the batched solver: training data and held-out points
+    Y, t_data = sph_surrogate.solve_points(pts, nsteps, args.precision, local)
+    X = sph_surrogate.features_of(pts)
+    Xtr, Ytr, Xte, Yte = X[:ntrain], Y[:ntrain], X[ntrain:], Y[ntrain:]
+    sur = sph_surrogate.Surrogate(heads=5, seed=0, device=local)
+    t0 = time.perf_counter()
+    sur.fit(Xtr, Ytr, steps=args.sweep_train_steps, lr=1e-3)
+    t_train = time.perf_counter() - t0
+    mean_te, route_te = sur.predict(Xte)
+    # 65,536 queries: predicted, the disagreeing ones re-solved
+    Xq = sph_surrogate.features_of(queries)
+    t0 = time.perf_counter()
+    mean_q, route_q = sur.predict(Xq)
+    t_pred = time.perf_counter() - t0
+    routed = [queries[k] for k in np.nonzero(route_q)[0]]
+    _, t_fallback = sph_surrogate.solve_points(routed, nsteps, args.precision, local) if routed \
+        else (None, 0.0)
+    line = sweep_line(args, nsteps, ntrain, nquery, t_one, t_data, len(pts), t_train, t_pred,
+                      t_fallback, mean_te, route_te, Yte, Ytr, route_q)
+    print(json.dumps(line))
+    return 0
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
-    ap.add_argument("--workload", default="couette3d", choices=["couette3d", "ensemble512"],
-                    help="couette3d: the headline 128^3 box; ensemble512: the batched sweep")
+    ap.add_argument("--sweep-steps", type=int, default=2000)
+    ap.add_argument("--sweep-train", type=int, default=20480)
+    ap.add_argument("--sweep-train-steps", type=int, default=3000)
+    ap.add_argument("--workload", default="couette3d",
+                    choices=["couette3d", "ensemble512", "sweep"],
+                    help="couette3d: the headline 128^3 box; ensemble512: 512 batched boxes; "
+                         "sweep: sweep points per hour with the surrogate")
     ap.add_argument("--steps", type=int, default=50)
     ap.add_argument("--warmup", type=int, default=5)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
-    ap.add_argument("--precision", default="fp64", choices=["fp64", "mixed"])
+    ap.add_argument("--precision", default=None, choices=["fp64", "mixed"],
+                    help="default: fp64 (the reference's precision); mixed for --workload sweep")
     ap.add_argument("--profile-steps", type=int, default=5)
     ap.add_argument("--e2e-steps", type=int, default=20)
     ap.add_argument("--pairs-traffic", type=float, default=None,
@@ -418,6 +522,8 @@ def main():
     ap.add_argument("--lattice", type=int, default=128,
                     help="lattice side; 128 is the benchmark, smaller sizes only for ncu captures")
     args = ap.parse_args()
+    if args.precision is None:
+        args.precision = "mixed" if args.workload == "sweep" else "fp64"
     if args.lattice != 128:
         global WORKLOAD_NAME
         WORKLOAD_NAME = "couette3d_%d (profiling size, not the benchmark)" % args.lattice
@@ -426,6 +532,14 @@ def main():
         args.warmup = 3
     world, rank, local, dist = dist_setup(args)
     try:
+        if args.workload == "sweep":
+            if args.impl == "reference":
+                if rank == 0:
+                    print(json.dumps({"impl": "reference", "unavailable":
+                                      "the reference has no batched solver or surrogate; its "
+                                      "one-box figure is the couette3d reference arm"}))
+                return 0
+            return run_sweep_bench(args, world, rank, local, dist)
         if args.workload == "ensemble512":
             if args.impl == "reference":
                 if rank == 0:

@@ -30,13 +30,17 @@ FEATURES = ["Wi", "omega_tau", "phi", "F0_ratio", "Vwall", "nkT"]
 FIXED = dict(dt=2e-5, eta=0.1, c=10.0, P0=0.0, rho=1.0, zeta=0.0, kT=0.01, F0_repulsion=1e-3)
 
 
-def draw_points(n, seed=0):
-    """n sweep points: dicts with the box side N and the sampled physical parameters."""
+def draw_points(n, seed=0, fixed_N=None, coll_seed=None):
+    """n sweep points: dicts with the box side N and the sampled physical parameters.
+    fixed_N and coll_seed pin the resolution and the colloid placement sequence (the
+    first k colloids of every point then sit at the same places), which makes the
+    observables functions of the six physical inputs alone (the surrogate's sweeps)."""
     rng = np.random.default_rng(seed)
     pts = []
     for _ in range(n):
+        N = int(rng.integers(32, 129))
         pts.append(dict(
-            N=int(rng.integers(32, 129)),
+            N=int(fixed_N) if fixed_N else N,
             tau=float(10 ** rng.uniform(-1, 1)),
             omega_tau=float(10 ** rng.uniform(-1, 1)),
             ncoll=int(rng.integers(0, 25)),
@@ -45,6 +49,8 @@ def draw_points(n, seed=0):
             nkT=float(rng.uniform(0.5, 2.0)),
             seed=int(rng.integers(0, 2 ** 31 - 1)),
         ))
+        if coll_seed is not None:
+            pts[-1]["seed"] = int(coll_seed)
     return pts
 
 

@@ -184,3 +184,43 @@ class Surrogate:
         spread = P[:, :, target].max(0) - P[:, :, target].min(0)
         scale = np.maximum(np.abs(mean[:, target]), 1e-12)
         return mean, spread / scale > tol
+
+
+# ---- sweeps: the solver as data source and fallback ----
+
+def solve_points(points, nsteps, precision="mixed", device=0, batch=512, observe_every=20,
+                 warm_frac=0.25):
+    """Observables (n x 4) of sweep points from the batched solver, `batch` boxes per
+    context; the averages skip the first warm_frac of the steps.  Returns (Y, seconds of
+    context creation + stepping)."""
+    import os
+    import tempfile
+    import time
+
+    import sph_ensemble
+
+    Y = np.zeros((len(points), OUT))
+    secs = 0.0
+    for c0 in range(0, len(points), batch):
+        chunk = points[c0:c0 + batch]
+        with tempfile.TemporaryDirectory() as wd:
+            paths, _ = sph_ensemble.write_inputs(chunk, os.path.join(wd, "in"), nsteps=nsteps)
+            t0 = time.perf_counter()
+            s = sph_b200.System(paths, precision=precision, device=device)
+            obs, _ = sph_ensemble.run_sweep(s, nsteps, observe_every,
+                                            warm=int(warm_frac * nsteps))
+            s.close()
+            secs += time.perf_counter() - t0
+        Y[c0:c0 + len(chunk)] = obs
+    return Y, secs
+
+
+def features_of(points):
+    import sph_ensemble
+
+    return np.stack([sph_ensemble.features(p, sph_ensemble.box_spec(p)) for p in points])
+
+
+def relative_error(pred, true):
+    """Wall-stress error measure: mean |pred - true| over mean |true| (normalised MAE)."""
+    return float(np.mean(np.abs(pred - true)) / max(np.mean(np.abs(true)), 1e-300))
