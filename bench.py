@@ -499,6 +499,57 @@ def run_sweep_bench(args, world, rank, local, dist):
     return 0
 
 
+def run_surrogate_train(args, world, rank, local, dist):
+    """Training throughput of the surrogate network (5 heads, batch 1024) on its tensor-core
+    kernels: samples per second and the dense FLOP rate of the training step."""
+    import torch
+
+    import sph_surrogate
+
+    if world > 1 and rank != 0:
+        return 0
+    heads, B = 5, 1024
+    net = sph_surrogate.MLP(heads=heads, max_batch=B, seed=0, device=local)
+    g = torch.Generator(device="cuda:%d" % local).manual_seed(0)
+    x = torch.randn(B, 6, generator=g, device="cuda:%d" % local)
+    y = torch.randn(B, 4, generator=g, device="cuda:%d" % local)
+    for _ in range(args.warmup):
+        net.train_step(x, y, 1e-3)
+    net.synchronize()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    with ClockSampler(local) as clk:
+        e0.record()  # the network runs on the legacy default stream, as torch does here
+        for _ in range(args.steps):
+            net.train_step(x, y, 1e-3)
+        e1.record()
+        e1.synchronize()
+    ms = e0.elapsed_time(e1)
+    # multiply-adds per sample and head: forward 6*256 + 2*256*256 + 256*4; the backward
+    # pass twice that (input and weight gradients), the 6-wide input gradient excepted
+    fwd = 6 * 256 + 2 * 256 * 256 + 256 * 4
+    flops = 2.0 * 3 * fwd * B * heads * args.steps
+    tf = flops / (ms * 1e-3) / 1e12
+    peak = None
+    path = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    if os.path.exists(path):
+        with open(path) as f:
+            peak = float(json.load(f).get("bf16_tflops", 0.0)) or None
+    line = {"metric": "surrogate training samples/s (5 heads, batch 1024)",
+            "value": B * args.steps / (ms * 1e-3), "unit": "samples/s", "n_gpus": 1,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms / args.steps,
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+            "dtype": "bf16 (fp32 accumulate)", "data": "synthetic",
+            "config": {"workload": "surrogate network 6-256-256-256-4, 5 heads, Adam"},
+            "roofline": {"bound": "tensor", "achieved": tf, "peak": peak, "unit": "TFLOP/s",
+                         "frac": tf / peak if peak else None, "traffic": None,
+                         "note": "1024 x 256 x 256 GEMMs: a step is a few microseconds of "
+                                 "tensor work and is launch- and latency-bound"},
+            "clocks": clk.summary()}
+    net.close()
+    print(json.dumps(line))
+    return 0
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -506,9 +557,10 @@ def main():
     ap.add_argument("--sweep-train", type=int, default=20480)
     ap.add_argument("--sweep-train-steps", type=int, default=3000)
     ap.add_argument("--workload", default="couette3d",
-                    choices=["couette3d", "ensemble512", "sweep"],
+                    choices=["couette3d", "ensemble512", "sweep", "surrogate"],
                     help="couette3d: the headline 128^3 box; ensemble512: 512 batched boxes; "
-                         "sweep: sweep points per hour with the surrogate")
+                         "sweep: sweep points per hour with the surrogate; surrogate: the "
+                         "network's training throughput")
     ap.add_argument("--steps", type=int, default=50)
     ap.add_argument("--warmup", type=int, default=5)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
@@ -532,6 +584,13 @@ def main():
         args.warmup = 3
     world, rank, local, dist = dist_setup(args)
     try:
+        if args.workload == "surrogate":
+            if args.impl == "reference":
+                if rank == 0:
+                    print(json.dumps({"impl": "reference", "unavailable":
+                                      "the reference has no learned component"}))
+                return 0
+            return run_surrogate_train(args, world, rank, local, dist)
         if args.workload == "sweep":
             if args.impl == "reference":
                 if rank == 0:
