@@ -569,11 +569,16 @@ def main():
     ap.add_argument("--profile-steps", type=int, default=5)
     ap.add_argument("--e2e-steps", type=int, default=20)
     ap.add_argument("--pairs-traffic", type=float, default=None,
-                    help="ncu dram bytes per k_pairs launch, if measured")
+                    help="ncu DRAM bytes per k_pairs launch (default: the FP64 capture at "
+                         "96^3, 788.8 MB, scaled by particle count to the benchmark)")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--lattice", type=int, default=128,
                     help="lattice side; 128 is the benchmark, smaller sizes only for ncu captures")
     args = ap.parse_args()
+    if args.pairs_traffic is None and args.lattice == 128 and args.precision in (None, "fp64"):
+        # dram__bytes_read.sum + dram__bytes_write.sum of one k_pairs launch at 96^3
+        # (940,032 particles), scaled to the 2,195,456 particles of the benchmark
+        args.pairs_traffic = (722.530304e6 + 66.258944e6) * 2195456 / 940032
     if args.precision is None:
         args.precision = "mixed" if args.workload == "sweep" else "fp64"
     if args.lattice != 128:
