@@ -241,6 +241,7 @@ def run_ours(args, world, rank, local, dist):
         path = write_workload(wd, args.lattice)
         sysm = sph_b200.System(path, precision=args.precision, device=local)
         n = sysm.N
+        tuning = sysm.autotune()
         sysm.step(args.warmup)
         sysm.synchronize()
         if dist is not None:
@@ -290,6 +291,7 @@ def run_ours(args, world, rank, local, dist):
         "data": "synthetic (lattice initial state)",
         "config": {"workload": WORKLOAD_NAME, "particles": n, "precision": args.precision,
                    "parallelism": "replicas only" if world > 1 else "single box",
+                   "launch_geometry": tuning,
                    "l2": "inputs larger than L2 (state ~0.7 GB > 126 MB), no flush",
                    "timing": "CUDA events around sph_step(K) on the engine stream, max over ranks"},
         "roofline": {"kernel": "k_pairs (fused velocity gradient, forces, dc/dt)",
@@ -344,6 +346,7 @@ def run_ensemble(args, world, rank, local, dist):
         paths, _ = sph_ensemble.write_inputs([pts[b] for b in mine], wd)
         sysm = sph_b200.System(paths, precision=args.precision, device=local)
         n = sysm.N
+        tuning = sysm.autotune()
         sysm.step(args.warmup)
         sysm.synchronize()
         if dist is not None:
@@ -395,6 +398,7 @@ def run_ensemble(args, world, rank, local, dist):
                    "precision": args.precision,
                    "parallelism": ("%d boxes on this rank of %d (sharded by particle-steps)"
                                    % (nb_mine, world)) if world > 1 else "one context",
+                   "launch_geometry": tuning,
                    "timing": "CUDA events around sph_step(K), max over ranks"},
         "e2e": {"value": n_all * e2e_steps / e2e_dt, "unit": UNIT, "h2d_bytes_per_step": 0,
                 "d2h_bytes_per_step": 512 * 4 * 8, "steps": e2e_steps},

@@ -259,6 +259,26 @@ sph_status sph_observe(sph_ctx* ctx);
 sph_status sph_observables(sph_ctx* ctx, double* host_out, long long* nsamples);
 sph_status sph_reset_observables(sph_ctx* ctx);
 
+/* Launch geometry of the neighbour passes (no reference counterpart; results do not
+   depend on it, bit for bit):
+     list_threads_per_cell  32: a warp per cell in the list build; 16: a half-warp per
+                            cell (2D cells at overlap 4 hold about 16 particles)
+     density_block          threads per block of the density pass: 64, 128 or 256
+   sph_set_tuning applies a geometry (captured step graphs are rebuilt).  sph_autotune
+   times the candidates on the context's current state -- the timed passes recompute the
+   same lists and densities, so the simulation is unchanged -- and keeps the fastest.
+   With cache_path it first looks for an entry keyed by GPU name, dimension, overlap and
+   particle count (rounded to a power of two) in that JSON file, and records its choice
+   there otherwise.  The cell size stays the reference's (rcut): its cell grid carries the
+   stale-range semantics of the exported cell arrays. */
+typedef struct sph_tuning {
+  int list_threads_per_cell;
+  int density_block;
+} sph_tuning;
+sph_status sph_get_tuning(const sph_ctx* ctx, sph_tuning* out);
+sph_status sph_set_tuning(sph_ctx* ctx, const sph_tuning* tuning);
+sph_status sph_autotune(sph_ctx* ctx, const char* cache_path, sph_tuning* chosen);
+
 /* Device time of the most recent sph_step, in milliseconds, measured with CUDA events
    on the context's stream. */
 sph_status sph_last_step_ms(sph_ctx* ctx, double* ms);

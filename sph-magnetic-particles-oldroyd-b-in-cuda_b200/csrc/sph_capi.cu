@@ -7,6 +7,8 @@
 #include <cmath>
 #include <cstdio>
 #include <cstring>
+#include <fstream>
+#include <sstream>
 #include <string>
 #include <vector>
 
@@ -45,6 +47,7 @@ struct sph_ctx {
   double last_ms = 0.0;
   int max_coll = 0;
   int cap_grown = 0;
+  sph_tuning tune = {32, 128};  // launch geometry (sph_set_tuning / sph_autotune)
 };
 
 namespace {
@@ -77,6 +80,8 @@ Launch launcher(sph_ctx* c) {
   L.prec = c->prec;
   L.stream = c->stream;
   L.launches = &c->launches;
+  L.list_tpc = c->tune.list_threads_per_cell;
+  L.density_block = c->tune.density_block;
   return L;
 }
 
@@ -1113,6 +1118,171 @@ sph_status sph_load_checkpoint(sph_ctx* c, const char* path) {
   c->gradv_valid = false;
   c->pos_dirty = true;
   drop_graphs(c);
+  return SPH_OK;
+}
+
+}  // extern "C"
+
+// ---- launch geometry and the autotuner ----
+namespace {
+
+bool tuning_ok(const sph_tuning& t) {
+  return (t.list_threads_per_cell == 32 || t.list_threads_per_cell == 16) &&
+         (t.density_block == 64 || t.density_block == 128 || t.density_block == 256);
+}
+
+// Cache key: GPU name, dimension, overlap of the first box, total particles rounded to a
+// power of two.
+std::string tune_key(const sph_ctx* c) {
+  cudaDeviceProp prop;
+  std::string name = cudaGetDeviceProperties(&prop, c->device) == cudaSuccess ? prop.name : "gpu";
+  for (char& ch : name)
+    if (ch == '"' || ch == '\\') ch = '_';
+  int lg = 0;
+  while ((1ll << (lg + 1)) <= (long long)std::max(c->d.Ntot, 1)) ++lg;
+  if ((1ll << (lg + 1)) - c->d.Ntot < c->d.Ntot - (1ll << lg)) ++lg;
+  char buf[320];
+  std::snprintf(buf, sizeof(buf), "%s|dim=%d|overlap=%g|N=2^%d", name.c_str(), c->dim,
+                c->boxes.empty() ? 0.0 : c->boxes[0].in.overlap, lg);
+  return buf;
+}
+
+// The cache file is a JSON object with one entry per line:
+//   "<key>": {"list_threads_per_cell": 16, "density_block": 128, "lists_ms": .., "density_ms": ..},
+bool cache_lookup(const char* path, const std::string& key, sph_tuning* t) {
+  std::ifstream f(path);
+  if (!f) return false;
+  const std::string head = "\"" + key + "\":";
+  std::string line;
+  while (std::getline(f, line)) {
+    const size_t a = line.find(head);
+    if (a == std::string::npos) continue;
+    sph_tuning r{0, 0};
+    const size_t p1 = line.find("\"list_threads_per_cell\":", a);
+    const size_t p2 = line.find("\"density_block\":", a);
+    if (p1 == std::string::npos || p2 == std::string::npos) return false;
+    r.list_threads_per_cell = std::atoi(line.c_str() + p1 + 24);
+    r.density_block = std::atoi(line.c_str() + p2 + 16);
+    if (!tuning_ok(r)) return false;
+    *t = r;
+    return true;
+  }
+  return false;
+}
+
+bool cache_store(const char* path, const std::string& key, const sph_tuning& t, double lists_ms,
+                 double density_ms) {
+  std::vector<std::string> keep;
+  {
+    std::ifstream f(path);
+    std::string line;
+    const std::string head = "\"" + key + "\":";
+    while (f && std::getline(f, line)) {
+      const size_t q = line.find('"');
+      if (q == std::string::npos || line.find(head) != std::string::npos) continue;
+      while (!line.empty() && (line.back() == ',' || line.back() == ' ' || line.back() == '\r'))
+        line.pop_back();
+      keep.push_back(line);
+    }
+  }
+  char entry[512];
+  std::snprintf(entry, sizeof(entry),
+                "\"%s\": {\"list_threads_per_cell\": %d, \"density_block\": %d, "
+                "\"lists_ms\": %.4f, \"density_ms\": %.4f}",
+                key.c_str(), t.list_threads_per_cell, t.density_block, lists_ms, density_ms);
+  keep.push_back(entry);
+  const std::string tmp = std::string(path) + ".tmp";
+  {
+    std::ofstream o(tmp);
+    if (!o) return false;
+    o << "{\n";
+    for (size_t k = 0; k < keep.size(); ++k) o << keep[k] << (k + 1 < keep.size() ? ",\n" : "\n");
+    o << "}\n";
+    if (!o) return false;
+  }
+  return std::rename(tmp.c_str(), path) == 0;
+}
+
+// Mean device time (ms) of `reps` launches of one phase after one warm-up launch.
+template <typename F>
+double time_phase(sph_ctx* c, int reps, F launch, bool* bad) {
+  cudaEvent_t e0, e1;
+  cudaEventCreate(&e0);
+  cudaEventCreate(&e1);
+  *bad |= launch() != 0;
+  cudaEventRecord(e0, c->stream);
+  for (int r = 0; r < reps; ++r) *bad |= launch() != 0;
+  cudaEventRecord(e1, c->stream);
+  cudaEventSynchronize(e1);
+  float ms = 0.f;
+  cudaEventElapsedTime(&ms, e0, e1);
+  cudaEventDestroy(e0);
+  cudaEventDestroy(e1);
+  return ms / reps;
+}
+
+}  // namespace
+
+extern "C" {
+
+sph_status sph_get_tuning(const sph_ctx* c, sph_tuning* out) {
+  if (!c || !out) return SPH_ERR_STATE;
+  *out = c->tune;
+  return SPH_OK;
+}
+
+sph_status sph_set_tuning(sph_ctx* c, const sph_tuning* t) {
+  CTX_GUARD(c);
+  if (!t || !tuning_ok(*t)) return fail(c, SPH_ERR_STATE, "unsupported launch geometry");
+  c->tune = *t;
+  drop_graphs(c);  // the captured steps carry the old geometry
+  return SPH_OK;
+}
+
+sph_status sph_autotune(sph_ctx* c, const char* cache_path, sph_tuning* chosen) {
+  CTX_GUARD(c);
+  if (c->in_step) return fail(c, SPH_ERR_STATE, "autotune inside a half-finished step");
+  const std::string key = tune_key(c);
+  sph_tuning t;
+  if (cache_path && cache_lookup(cache_path, key, &t)) {
+    sph_status s = sph_set_tuning(c, &t);
+    if (s == SPH_OK && chosen) *chosen = t;
+    return s;
+  }
+  // valid lists for the current positions; both timed phases recompute the same values
+  // from the current state, so tuning leaves the simulation where it was
+  sph_status s = ensure_lists(c);
+  if (s != SPH_OK) return s;
+  const int reps = c->d.Ntot > (1 << 20) ? 3 : 10;
+  bool bad = false;
+  sph_tuning best = c->tune;
+  double best_lists = 1e300, best_dens = 1e300;
+  for (int tpc : {32, 16}) {
+    Launch L = launcher(c);
+    L.list_tpc = tpc;
+    const double ms = time_phase(c, reps, [&] { return launch_build_lists_dim(L, c->dim); }, &bad);
+    if (ms < best_lists) {
+      best_lists = ms;
+      best.list_threads_per_cell = tpc;
+    }
+  }
+  for (int nt : {64, 128, 256}) {
+    Launch L = launcher(c);
+    L.density_block = nt;
+    const double ms = time_phase(c, reps, [&] { return launch_density_dim(L, c->dim); }, &bad);
+    if (ms < best_dens) {
+      best_dens = ms;
+      best.density_block = nt;
+    }
+  }
+  if (bad) return cuda_fail(c, "autotune");
+  s = check_device(c);
+  if (s != SPH_OK) return s;
+  s = sph_set_tuning(c, &best);
+  if (s != SPH_OK) return s;
+  if (cache_path && !cache_store(cache_path, key, best, best_lists, best_dens))
+    return fail(c, SPH_ERR_IO, "cannot write the autotune cache");
+  if (chosen) *chosen = best;
   return SPH_OK;
 }
 

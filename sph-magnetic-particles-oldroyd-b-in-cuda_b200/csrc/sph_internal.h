@@ -175,6 +175,9 @@ struct Launch {
   int prec;  // sph_precision
   void* stream;
   long long* launches;
+  int list_tpc = 32;        // threads per cell of the list build (32 or 16)
+  int density_block = 128;  // threads per block of the density pass (64, 128 or 256)
+  // (launch geometry only: results do not depend on it)
 };
 
 enum PairMode { kPairFused = 0, kPairGradvAll = 1, kPairForcesOnly = 2 };

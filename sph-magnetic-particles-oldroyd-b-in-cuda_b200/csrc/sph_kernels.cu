@@ -322,28 +322,45 @@ __device__ __forceinline__ void density_epilogue(const Dev& d, int i, const BoxP
 // (Summing the density over the hits inside this kernel was measured slower than the
 // separate k_density pass: the per-lane hit loops diverge and the warp runs the FP64
 // kernel evaluation for its busiest lane.)
+//
+// TPC (threads per cell) is 32 or 16.  With 16, each half-warp works on its own cell:
+// 2D cells at overlap 4 hold about 16 particles, so a whole warp per cell leaves half of
+// its lanes idle.  The lists are the same either way (same candidates, same order).
 constexpr int kListWarps = 8;
 
-template <int DIM>
+template <int DIM, int TPC>
 __global__ void __launch_bounds__(kListWarps * 32) k_build_lists(Dev d) {
+  static_assert(TPC == 32 || TPC == 16, "a warp or a half-warp per cell");
   __shared__ float4 stage[kListWarps][32];
   const int w = threadIdx.x >> 5, lane = threadIdx.x & 31;
-  const int cell = blockIdx.x * kListWarps + w;
-  if (cell >= d.Ctot) return;
-  const int b = d.cell_box[cell];
+  const int sub = lane / TPC, gl = lane % TPC;  // group within the warp, lane within the group
+  float4* st = &stage[w][sub * TPC];
+  const int cell = (blockIdx.x * kListWarps + w) * (32 / TPC) + sub;
+  // both groups of a warp walk the same loop structure in lockstep (divergent halves would
+  // run one after the other): trip counts are warp maxima, a group past its own range idles
+  const bool live = cell < d.Ctot;
+  if (!__any_sync(SPH_FULL, live)) return;
+  const int cl = live ? cell : 0;
+  const int b = d.cell_box[cl];
   const BoxParams& p = d.box[b];
   const int N0 = p.Ncells[0], N1 = p.Ncells[1], N2 = p.Ncells[2];
-  const int lc = cell - p.cell0;
+  const int lc = cl - p.cell0;
   const int cx = lc % N0, cy = (lc / N0) % N1, cz = DIM == 3 ? lc / (N0 * N1) : 0;
-  const int beg = d.cell_begin[cell], end = d.cell_begin[cell + 1];
+  const int beg = live ? d.cell_begin[cl] : 0, end = live ? d.cell_begin[cl + 1] : 0;
   const double ox = cx * p.cell_size[0];
   const double oy = cy * p.cell_size[1] - (p.wall ? p.wall_width : 0.0);
   const double oz = DIM == 3 ? cz * p.cell_size[2] : 0.0;
   const float cut2 = (float)p.list_cut2;
   const int cap = d.cap;
+  auto warp_max = [](int v) {
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) v = max(v, __shfl_xor_sync(SPH_FULL, v, o));
+    return v;
+  };
+  const int span = warp_max(end - beg);
   int maxcnt = 0;
-  for (int t0 = beg; t0 < end; t0 += 32) {
-    const int i = t0 + lane;
+  for (int t0 = 0; t0 < span; t0 += TPC) {
+    const int i = beg + t0 + gl;
     const bool active = i < end;
     float xi = 0.f, yi = 0.f, zi = 0.f;
     bool odd = false, lost = false;
@@ -362,6 +379,8 @@ __global__ void __launch_bounds__(kListWarps * 32) k_build_lists(Dev d) {
         raise_status(d, finite ? kStatCellRange : kStatNaN, d.gid[i]);
       }
     }
+    const bool listed = active && !odd && !lost;
+    int* rowp = d.nbr + (size_t)(active ? i : 0) * cap;
     int cnt = 0;
     for (int ddx = -1; ddx <= 1; ++ddx)
       for (int ddy = -1; ddy <= 1; ++ddy)
@@ -378,24 +397,46 @@ __global__ void __launch_bounds__(kListWarps * 32) k_build_lists(Dev d) {
             if (ny < 0) { ny += N1; sy = -p.L[1]; }
             if (ny >= N1) { ny -= N1; sy = p.L[1]; }
           }
-          if (ny < 0 || ny >= N1) continue;
-          const int nc = p.cell0 + (DIM == 3 ? (nz * N1 + ny) * N0 + nx : ny * N0 + nx);
-          const int s = d.cell_start[nc] + p.slot0, e = d.cell_end[nc] + p.slot0;
-          for (int c0 = s; c0 <= e; c0 += 32) {
-            const int j = c0 + lane;
-            if (j <= e) {
+          // an empty range where the neighbour row does not exist (walls) or the group idles
+          int s = 0, e = -1;
+          if (live && ny >= 0 && ny < N1) {
+            const int nc = p.cell0 + (DIM == 3 ? (nz * N1 + ny) * N0 + nx : ny * N0 + nx);
+            s = d.cell_start[nc] + p.slot0;
+            e = d.cell_end[nc] + p.slot0;
+          }
+          const int nch = e >= s ? (e - s + TPC) / TPC : 0;
+          const int nchw = TPC == 32 ? nch : warp_max(nch);
+          for (int k = 0; k < nchw; ++k) {
+            const int c0 = s + k * TPC;
+            const int j = c0 + gl;
+            if (k < nch && j <= e) {
               double4 xj = d.pos[j];
-              stage[w][lane] = make_float4((float)(xj.x + sx - ox), (float)(xj.y + sy - oy),
-                                           (float)(xj.z + sz - oz), __int_as_float(j));
+              st[gl] = make_float4((float)(xj.x + sx - ox), (float)(xj.y + sy - oy),
+                                   (float)(xj.z + sz - oz), __int_as_float(j));
             }
             __syncwarp();
-            const int n = min(32, e - c0 + 1);
-            if (active && !odd && !lost) {
-              // hit mask of this chunk, branch-free; staged candidate q is slot c0 + q
-              unsigned hits = 0u;
+            const int n = k < nch ? min(TPC, e - c0 + 1) : 0;
+            // hit mask of this chunk, branch-free; staged candidate q is slot c0 + q
+            unsigned hits = 0u;
+            if (TPC == 32) {
+              if (listed) {
 #pragma unroll 4
-              for (int q = 0; q < n; ++q) {
-                const float4 c = stage[w][q];
+                for (int q = 0; q < n; ++q) {
+                  const float4 c = st[q];
+                  const float rx = xi - c.x, ry = yi - c.y;
+                  float r2 = rx * rx + ry * ry;
+                  if (DIM == 3) {
+                    const float rz = zi - c.z;
+                    r2 += rz * rz;
+                  }
+                  hits |= (r2 < cut2 ? 1u : 0u) << q;
+                }
+              }
+            } else {
+              // a fixed trip count keeps both halves on one instruction stream
+#pragma unroll
+              for (int q = 0; q < TPC; ++q) {
+                const float4 c = st[q];
                 const float rx = xi - c.x, ry = yi - c.y;
                 float r2 = rx * rx + ry * ry;
                 if (DIM == 3) {
@@ -404,14 +445,14 @@ __global__ void __launch_bounds__(kListWarps * 32) k_build_lists(Dev d) {
                 }
                 hits |= (r2 < cut2 ? 1u : 0u) << q;
               }
-              // append in candidate order to the particle's own list row
-              int* rowp = d.nbr + (size_t)i * cap;
-              while (hits) {
-                const int q = __ffs(hits) - 1;
-                hits &= hits - 1u;
-                if (cnt < cap) rowp[cnt] = c0 + q;
-                ++cnt;
-              }
+              hits &= (listed && n > 0) ? (0xFFFFFFFFu >> (32 - n)) : 0u;
+            }
+            // append in candidate order to the particle's own list row
+            while (hits) {
+              const int q = __ffs(hits) - 1;
+              hits &= hits - 1u;
+              if (cnt < cap) rowp[cnt] = c0 + q;
+              ++cnt;
             }
             __syncwarp();
           }
@@ -420,18 +461,24 @@ __global__ void __launch_bounds__(kListWarps * 32) k_build_lists(Dev d) {
       d.nbr_cnt[i] = cnt;
       maxcnt = max(maxcnt, cnt);
     }
-    // particles exactly on the upper box edge: their own neighbour cells
+    // particles exactly on the upper box edge: their own neighbour cells, the whole warp
+    // testing one such particle's candidates at a time
     unsigned odd_mask = __ballot_sync(SPH_FULL, active && odd);
     while (odd_mask) {
       const int l = __ffs(odd_mask) - 1;
       odd_mask &= odd_mask - 1;
-      const int ti = t0 + l;
+      // the particle and its cell's geometry, from the lane that holds it
+      const int ti = __shfl_sync(SPH_FULL, i, l);
+      const int tb = __shfl_sync(SPH_FULL, b, l);
+      const BoxParams& tp = d.box[tb];
       const double4 xt = d.pos[ti];
       int ax = 0, ay = 0, az = 0;
-      if (!own_cell(p, xt.x, xt.y, xt.z, ax, ay, az)) continue;  // checked above: cannot fail
-      const double tox = ax * p.cell_size[0];
-      const double toy = ay * p.cell_size[1] - (p.wall ? p.wall_width : 0.0);
-      const double toz = DIM == 3 ? az * p.cell_size[2] : 0.0;
+      own_cell(tp, xt.x, xt.y, xt.z, ax, ay, az);  // checked above: cannot fail
+      const int M0 = tp.Ncells[0], M1 = tp.Ncells[1], M2 = tp.Ncells[2];
+      const double tox = ax * tp.cell_size[0];
+      const double toy = ay * tp.cell_size[1] - (tp.wall ? tp.wall_width : 0.0);
+      const double toz = DIM == 3 ? az * tp.cell_size[2] : 0.0;
+      const float tcut2 = (float)tp.list_cut2;
       const float txi = (float)(xt.x - tox), tyi = (float)(xt.y - toy), tzi = (float)(xt.z - toz);
       int tcnt = 0;
       for (int ddx = -1; ddx <= 1; ++ddx)
@@ -439,19 +486,19 @@ __global__ void __launch_bounds__(kListWarps * 32) k_build_lists(Dev d) {
           for (int ddz = (DIM == 3 ? -1 : 0); ddz <= (DIM == 3 ? 1 : 0); ++ddz) {
             int nx = ax + ddx, ny = ay + ddy, nz = az + ddz;
             double sx = 0.0, sy = 0.0, sz = 0.0;
-            if (nx < 0) { nx += N0; sx = -p.L[0]; }
-            if (nx >= N0) { nx -= N0; sx = p.L[0]; }
+            if (nx < 0) { nx += M0; sx = -tp.L[0]; }
+            if (nx >= M0) { nx -= M0; sx = tp.L[0]; }
             if (DIM == 3) {
-              if (nz < 0) { nz += N2; sz = -p.L[2]; }
-              if (nz >= N2) { nz -= N2; sz = p.L[2]; }
+              if (nz < 0) { nz += M2; sz = -tp.L[2]; }
+              if (nz >= M2) { nz -= M2; sz = tp.L[2]; }
             }
-            if (!p.wall) {
-              if (ny < 0) { ny += N1; sy = -p.L[1]; }
-              if (ny >= N1) { ny -= N1; sy = p.L[1]; }
+            if (!tp.wall) {
+              if (ny < 0) { ny += M1; sy = -tp.L[1]; }
+              if (ny >= M1) { ny -= M1; sy = tp.L[1]; }
             }
-            if (ny < 0 || ny >= N1) continue;
-            const int nc = p.cell0 + (DIM == 3 ? (nz * N1 + ny) * N0 + nx : ny * N0 + nx);
-            const int s = d.cell_start[nc] + p.slot0, e = d.cell_end[nc] + p.slot0;
+            if (ny < 0 || ny >= M1) continue;
+            const int nc = tp.cell0 + (DIM == 3 ? (nz * M1 + ny) * M0 + nx : ny * M0 + nx);
+            const int s = d.cell_start[nc] + tp.slot0, e = d.cell_end[nc] + tp.slot0;
             for (int c0 = s; c0 <= e; c0 += 32) {
               const int j = c0 + lane;
               bool hit = false;
@@ -464,7 +511,7 @@ __global__ void __launch_bounds__(kListWarps * 32) k_build_lists(Dev d) {
                   const float rz = tzi - (float)(xj.z + sz - toz);
                   r2 += rz * rz;
                 }
-                hit = r2 < cut2;
+                hit = r2 < tcut2;
               }
               const unsigned hits = __ballot_sync(SPH_FULL, hit);
               const int pos = tcnt + __popc(hits & ((1u << lane) - 1u));
@@ -477,8 +524,7 @@ __global__ void __launch_bounds__(kListWarps * 32) k_build_lists(Dev d) {
     }
   }
   // warp max of the counts -> capacity check
-#pragma unroll
-  for (int o = 16; o > 0; o >>= 1) maxcnt = max(maxcnt, __shfl_xor_sync(SPH_FULL, maxcnt, o));
+  maxcnt = warp_max(maxcnt);
   if (lane == 0 && maxcnt > 0) {
     atomicMax(&d.err_info[1], maxcnt);
     if (maxcnt > cap) atomicOr(d.status, (unsigned)kStatCapacity);
@@ -1193,11 +1239,16 @@ int launch_reorder(const Launch& L, bool permute_forces) {
 
 int launch_build_lists_dim(const Launch& L, int dim) {
   if (L.d.Ctot == 0) return 0;
-  const int nb = blocks(L.d.Ctot, kListWarps);
-  if (dim == 3)
-    k_build_lists<3><<<nb, kListWarps * 32, 0, S(L)>>>(L.d);
-  else
-    k_build_lists<2><<<nb, kListWarps * 32, 0, S(L)>>>(L.d);
+  const bool half = L.list_tpc == 16;
+  const int nb = blocks(L.d.Ctot, kListWarps * (half ? 2 : 1));
+  constexpr int nt = kListWarps * 32;
+  if (dim == 3) {
+    if (half) k_build_lists<3, 16><<<nb, nt, 0, S(L)>>>(L.d);
+    else k_build_lists<3, 32><<<nb, nt, 0, S(L)>>>(L.d);
+  } else {
+    if (half) k_build_lists<2, 16><<<nb, nt, 0, S(L)>>>(L.d);
+    else k_build_lists<2, 32><<<nb, nt, 0, S(L)>>>(L.d);
+  }
   return check(L);
 }
 
@@ -1209,13 +1260,14 @@ int launch_colloid_cells_n(const Launch& L, int nboxes, int max_coll) {
 
 int launch_density_dim(const Launch& L, int dim) {
   if (L.d.Ntot == 0) return 0;
-  const int nb = blocks(L.d.Ntot, kT);
+  const int nt = L.density_block;
+  const int nb = blocks(L.d.Ntot, nt);
   if (L.prec == SPH_PREC_FP64) {
-    if (dim == 3) k_density<double, 3><<<nb, kT, 0, S(L)>>>(L.d);
-    else k_density<double, 2><<<nb, kT, 0, S(L)>>>(L.d);
+    if (dim == 3) k_density<double, 3><<<nb, nt, 0, S(L)>>>(L.d);
+    else k_density<double, 2><<<nb, nt, 0, S(L)>>>(L.d);
   } else {
-    if (dim == 3) k_density<float, 3><<<nb, kT, 0, S(L)>>>(L.d);
-    else k_density<float, 2><<<nb, kT, 0, S(L)>>>(L.d);
+    if (dim == 3) k_density<float, 3><<<nb, nt, 0, S(L)>>>(L.d);
+    else k_density<float, 2><<<nb, nt, 0, S(L)>>>(L.d);
   }
   return check(L);
 }

@@ -8,7 +8,7 @@
 // writer thread; the GPU goes on with the next steps while the files are formatted.
 //
 //   sph_run [--input FILE] [--particles FILE] [--precision fp64|mixed] [--no-graph]
-//           [--steps N] [--checkpoint FILE] [--restart FILE] [--quiet]
+//           [--steps N] [--checkpoint FILE] [--restart FILE] [--autotune CACHE] [--quiet]
 #include <chrono>
 #include <condition_variable>
 #include <cstdio>
@@ -32,7 +32,7 @@ struct Args {
   int precision = SPH_PREC_FP64;
   bool graph = true;
   int steps = -1;  // -1: Nsteps of the input file
-  std::string checkpoint, restart;
+  std::string checkpoint, restart, autotune;
   bool quiet = false;
 };
 
@@ -63,6 +63,8 @@ bool parse_args(int argc, char** argv, Args* a) {
       if (!next(&a->checkpoint)) return false;
     } else if (s == "--restart") {
       if (!next(&a->restart)) return false;
+    } else if (s == "--autotune") {
+      if (!next(&a->autotune)) return false;
     } else if (s == "--quiet") {
       a->quiet = true;
     } else {
@@ -176,7 +178,7 @@ int main(int argc, char** argv) {
     std::fprintf(stderr,
                  "usage: sph_run [--input FILE] [--particles FILE] [--precision fp64|mixed]\n"
                  "               [--no-graph] [--steps N] [--checkpoint FILE] [--restart FILE]"
-                 " [--quiet]\n");
+                 " [--autotune CACHE] [--quiet]\n");
     return 2;
   }
   sph_input in;
@@ -213,6 +215,15 @@ int main(int argc, char** argv) {
   } else {
     s = sph_initial_forces(ctx);
     if (s != SPH_OK) return fail("initial forces", s, ctx);
+  }
+
+  if (!a.autotune.empty()) {
+    sph_tuning t;
+    s = sph_autotune(ctx, a.autotune.c_str(), &t);
+    if (s != SPH_OK) return fail("autotune", s, ctx);
+    if (!a.quiet)
+      std::printf("sph_run: launch geometry %d threads per cell, density blocks of %d\n",
+                  t.list_threads_per_cell, t.density_block);
   }
 
   std::vector<int> type((size_t)N);

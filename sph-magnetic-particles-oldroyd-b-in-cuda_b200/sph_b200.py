@@ -51,7 +51,8 @@ EXPORTS = [
     "sph_read_wall_forces", "sph_export_cells", "sph_export_colloid_cells",
     "sph_kinetic_energy", "sph_last_step_ms", "sph_kernel_launches", "sph_host_setup",
     "sph_profile_phases", "sph_phase_name", "sph_save_checkpoint", "sph_load_checkpoint",
-    "sph_observe", "sph_observables", "sph_reset_observables",
+    "sph_observe", "sph_observables", "sph_reset_observables", "sph_get_tuning",
+    "sph_set_tuning", "sph_autotune",
 ]
 OBSERVABLES = ["wall_stress", "N1", "chain_order", "kinetic_energy"]
 
@@ -79,6 +80,10 @@ class SphInput(ctypes.Structure):
 class SphOptions(ctypes.Structure):
     _fields_ = [("precision", c_int), ("device", c_int), ("use_graph", c_int),
                 ("nbr_capacity", c_int)]
+
+
+class SphTuning(ctypes.Structure):
+    _fields_ = [("list_threads_per_cell", c_int), ("density_block", c_int)]
 
 
 class SphInfo(ctypes.Structure):
@@ -156,6 +161,9 @@ def lib():
         L.sph_export_colloid_cells.argtypes = [c_void_p, PI, PI, PI, PI]
         L.sph_kinetic_energy.argtypes = [c_void_p, PD]
         L.sph_save_checkpoint.argtypes = [c_void_p, c_char_p]
+        L.sph_get_tuning.argtypes = [c_void_p, ctypes.POINTER(SphTuning)]
+        L.sph_set_tuning.argtypes = [c_void_p, ctypes.POINTER(SphTuning)]
+        L.sph_autotune.argtypes = [c_void_p, c_char_p, ctypes.POINTER(SphTuning)]
         L.sph_observe.argtypes = [c_void_p]
         L.sph_observables.argtypes = [c_void_p, PD, ctypes.POINTER(ctypes.c_longlong)]
         L.sph_reset_observables.argtypes = [c_void_p]
@@ -415,6 +423,23 @@ class System:
         out = np.zeros(self.nboxes, dtype=np.float64)
         self._ok(lib().sph_kinetic_energy(self._h, out.ctypes.data_as(PD)))
         return out
+
+    def tuning(self):
+        t = SphTuning()
+        self._ok(lib().sph_get_tuning(self._h, ctypes.byref(t)))
+        return {"list_threads_per_cell": t.list_threads_per_cell, "density_block": t.density_block}
+
+    def set_tuning(self, list_threads_per_cell=32, density_block=128):
+        t = SphTuning(list_threads_per_cell, density_block)
+        self._ok(lib().sph_set_tuning(self._h, ctypes.byref(t)))
+
+    def autotune(self, cache_path=None):
+        """Pick the fastest launch geometry (cached per GPU, dim, overlap and size when a
+        cache file is given); returns it.  The simulation state is not changed."""
+        t = SphTuning()
+        self._ok(lib().sph_autotune(self._h, os.fsencode(cache_path) if cache_path else None,
+                                    ctypes.byref(t)))
+        return {"list_threads_per_cell": t.list_threads_per_cell, "density_block": t.density_block}
 
     def observe(self):
         """Add one sample of every box's observables (asynchronous)."""
