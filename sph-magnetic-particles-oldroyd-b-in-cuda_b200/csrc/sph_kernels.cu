@@ -328,13 +328,61 @@ __device__ __forceinline__ void density_epilogue(const Dev& d, int i, const BoxP
 // its lanes idle.  The lists are the same either way (same candidates, same order).
 constexpr int kListWarps = 8;
 
+// Packed FP32 pairs (the f32x2 arithmetic of sm_100): two candidates per instruction.
+typedef unsigned long long f32x2;
+__device__ __forceinline__ f32x2 f2_pack(float lo, float hi) {
+  f32x2 d;
+  asm("mov.b64 %0, {%1, %2};" : "=l"(d) : "f"(lo), "f"(hi));
+  return d;
+}
+__device__ __forceinline__ f32x2 f2_sub(f32x2 a, f32x2 b) {
+  f32x2 d;
+  asm("sub.rn.f32x2 %0, %1, %2;" : "=l"(d) : "l"(a), "l"(b));
+  return d;
+}
+__device__ __forceinline__ f32x2 f2_mul(f32x2 a, f32x2 b) {
+  f32x2 d;
+  asm("mul.rn.f32x2 %0, %1, %2;" : "=l"(d) : "l"(a), "l"(b));
+  return d;
+}
+__device__ __forceinline__ f32x2 f2_fma(f32x2 a, f32x2 b, f32x2 c) {
+  f32x2 d;
+  asm("fma.rn.f32x2 %0, %1, %2, %3;" : "=l"(d) : "l"(a), "l"(b), "l"(c));
+  return d;
+}
+
+// Candidate test of two staged candidates against one particle: r2 < cut2 for each, as
+// the sign bit of r2 - cut2 (exact: the sign of a rounded difference is the sign of the
+// exact one), shifted into `hits` first candidate first.  Staged padding at 1e30 gives
+// r2 = +inf and no hit.
+template <int DIM>
+__device__ __forceinline__ unsigned list_test2(unsigned hits, f32x2 xi, f32x2 yi, f32x2 zi,
+                                               f32x2 cut2, float ax, float bx, float ay,
+                                               float by, float az, float bz) {
+  const f32x2 rx = f2_sub(xi, f2_pack(ax, bx)), ry = f2_sub(yi, f2_pack(ay, by));
+  f32x2 r2 = f2_fma(ry, ry, f2_mul(rx, rx));
+  if (DIM == 3) {
+    const f32x2 rz = f2_sub(zi, f2_pack(az, bz));
+    r2 = f2_fma(rz, rz, r2);
+  }
+  unsigned lo, hi;
+  asm("mov.b64 {%0, %1}, %2;" : "=r"(lo), "=r"(hi) : "l"(f2_sub(r2, cut2)));
+  hits = (hits << 1) | (lo >> 31);
+  return (hits << 1) | (hi >> 31);
+}
+
 template <int DIM, int TPC>
 __global__ void __launch_bounds__(kListWarps * 32) k_build_lists(Dev d) {
   static_assert(TPC == 32 || TPC == 16, "a warp or a half-warp per cell");
-  __shared__ float4 stage[kListWarps][32];
+  // candidates staged as three float rows per warp, read four at a time
+  __shared__ __align__(16) float stage_x[kListWarps][32];
+  __shared__ __align__(16) float stage_y[kListWarps][32];
+  __shared__ __align__(16) float stage_z[kListWarps][32];
   const int w = threadIdx.x >> 5, lane = threadIdx.x & 31;
   const int sub = lane / TPC, gl = lane % TPC;  // group within the warp, lane within the group
-  float4* st = &stage[w][sub * TPC];
+  float* stx = &stage_x[w][sub * TPC];
+  float* sty = &stage_y[w][sub * TPC];
+  float* stz = &stage_z[w][sub * TPC];
   const int cell = (blockIdx.x * kListWarps + w) * (32 / TPC) + sub;
   // both groups of a warp walk the same loop structure in lockstep (divergent halves would
   // run one after the other): trip counts are warp maxima, a group past its own range idles
@@ -380,6 +428,8 @@ __global__ void __launch_bounds__(kListWarps * 32) k_build_lists(Dev d) {
       }
     }
     const bool listed = active && !odd && !lost;
+    const f32x2 xi2 = f2_pack(xi, xi), yi2 = f2_pack(yi, yi), zi2 = f2_pack(zi, zi);
+    const f32x2 cut22 = f2_pack(cut2, cut2);
     int* rowp = d.nbr + (size_t)(active ? i : 0) * cap;
     int cnt = 0;
     for (int ddx = -1; ddx <= 1; ++ddx)
@@ -409,43 +459,37 @@ __global__ void __launch_bounds__(kListWarps * 32) k_build_lists(Dev d) {
           for (int k = 0; k < nchw; ++k) {
             const int c0 = s + k * TPC;
             const int j = c0 + gl;
+            float vx = 1e30f, vy = 1e30f, vz = 1e30f;  // padding: never a hit
             if (k < nch && j <= e) {
               double4 xj = d.pos[j];
-              st[gl] = make_float4((float)(xj.x + sx - ox), (float)(xj.y + sy - oy),
-                                   (float)(xj.z + sz - oz), __int_as_float(j));
+              vx = (float)(xj.x + sx - ox);
+              vy = (float)(xj.y + sy - oy);
+              vz = (float)(xj.z + sz - oz);
             }
+            stx[gl] = vx;
+            sty[gl] = vy;
+            if (DIM == 3) stz[gl] = vz;
             __syncwarp();
             const int n = k < nch ? min(TPC, e - c0 + 1) : 0;
-            // hit mask of this chunk, branch-free; staged candidate q is slot c0 + q
+            // hit mask of this chunk; staged candidate q is slot c0 + q.  A half-warp group
+            // runs a fixed trip count, which keeps both halves on one instruction stream.
+            const int m = TPC == 32 ? (n + 3) & ~3 : TPC;
             unsigned hits = 0u;
-            if (TPC == 32) {
-              if (listed) {
-#pragma unroll 4
-                for (int q = 0; q < n; ++q) {
-                  const float4 c = st[q];
-                  const float rx = xi - c.x, ry = yi - c.y;
-                  float r2 = rx * rx + ry * ry;
-                  if (DIM == 3) {
-                    const float rz = zi - c.z;
-                    r2 += rz * rz;
-                  }
-                  hits |= (r2 < cut2 ? 1u : 0u) << q;
-                }
+            if (TPC == 16 || listed) {
+#pragma unroll 2
+              for (int q = 0; q < m; q += 4) {
+                const float4 cx = *reinterpret_cast<const float4*>(stx + q);
+                const float4 cy = *reinterpret_cast<const float4*>(sty + q);
+                const float4 cz = DIM == 3 ? *reinterpret_cast<const float4*>(stz + q)
+                                           : make_float4(0.f, 0.f, 0.f, 0.f);
+                hits = list_test2<DIM>(hits, xi2, yi2, zi2, cut22, cx.x, cx.y, cy.x, cy.y, cz.x,
+                                       cz.y);
+                hits = list_test2<DIM>(hits, xi2, yi2, zi2, cut22, cx.z, cx.w, cy.z, cy.w, cz.z,
+                                       cz.w);
               }
-            } else {
-              // a fixed trip count keeps both halves on one instruction stream
-#pragma unroll
-              for (int q = 0; q < TPC; ++q) {
-                const float4 c = st[q];
-                const float rx = xi - c.x, ry = yi - c.y;
-                float r2 = rx * rx + ry * ry;
-                if (DIM == 3) {
-                  const float rz = zi - c.z;
-                  r2 += rz * rz;
-                }
-                hits |= (r2 < cut2 ? 1u : 0u) << q;
-              }
-              hits &= (listed && n > 0) ? (0xFFFFFFFFu >> (32 - n)) : 0u;
+              // first candidate was shifted in first: reverse into bit q = candidate q
+              hits = m > 0 ? __brev(hits) >> (32 - m) : 0u;
+              if (TPC == 16) hits &= (listed && n > 0) ? (0xFFFFFFFFu >> (32 - n)) : 0u;
             }
             // append in candidate order to the particle's own list row
             while (hits) {
