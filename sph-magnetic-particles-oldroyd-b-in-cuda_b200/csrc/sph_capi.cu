@@ -74,6 +74,22 @@ bool dalloc(sph_ctx* c, T** p, size_t n) {
   return true;
 }
 
+// Device buffers that live only while a context is being created.
+struct TmpDev {
+  std::vector<void*> bufs;
+  template <typename T>
+  bool alloc(T** p, size_t n) {
+    void* q = nullptr;
+    if (cudaMalloc(&q, std::max<size_t>(n, 1) * sizeof(T)) != cudaSuccess) return false;
+    bufs.push_back(q);
+    *p = static_cast<T*>(q);
+    return true;
+  }
+  ~TmpDev() {
+    for (void* q : bufs) cudaFree(q);
+  }
+};
+
 Launch launcher(sph_ctx* c) {
   Launch L;
   L.d = c->d;
@@ -382,11 +398,11 @@ sph_status sph_create_ensemble(int nboxes, const sph_input* inputs,
   c->use_graph = o.use_graph;
   c->nboxes = nboxes;
   c->boxes.resize(nboxes);
-  static thread_local std::string create_err;
+  const bool dev_init = o.init_on_device != 0;
   for (int b = 0; b < nboxes; ++b) {
     std::string m;
     sph_status s = build_box(inputs[b], particles_paths ? particles_paths[b] : nullptr,
-                             &c->boxes[b], &m);
+                             &c->boxes[b], &m, dev_init);
     if (s != SPH_OK) {
       fprintf(stderr, "sph_create: box %d: %s\n", b, m.c_str());
       delete c;
@@ -413,6 +429,96 @@ sph_status sph_create_ensemble(int nboxes, const sph_input* inputs,
   }
   cudaEventCreate(&c->ev0);
   cudaEventCreate(&c->ev1);
+  // ---- lattice boxes built on the device: count the kept and wall sites per block ----
+  TmpDev tmp;
+  std::vector<InitBox> ib;
+  std::vector<int> blk_box, ib_of_box(nboxes, -1), offs;
+  std::vector<double> centres;
+  InitBox* d_ib = nullptr;
+  int* d_blk_box = nullptr;
+  double* d_centres = nullptr;
+  if (dev_init) {
+    for (int b = 0; b < nboxes; ++b) {
+      const HostBox& hb = c->boxes[b];
+      if (!hb.lattice_on_device) continue;
+      const BoxParams& p = hb.p;
+      InitBox B{};
+      B.box = b;
+      B.dim = p.dim;
+      B.wall = p.wall;
+      for (int q = 0; q < 3; ++q) {
+        B.Nxyz[q] = hb.Nxyz[q];
+        B.dx[q] = hb.dx[q];
+        B.L[q] = p.L[q];
+      }
+      B.nsites = B.Nxyz[0] * B.Nxyz[1] * (p.dim == 3 ? B.Nxyz[2] : 1);
+      B.blk0 = (int)blk_box.size();
+      B.nblk = (B.nsites + kInitThreads - 1) / kInitThreads;
+      blk_box.insert(blk_box.end(), B.nblk, (int)ib.size());
+      B.coll0 = (int)centres.size() / 3;
+      B.ncoll = p.N_colloids;
+      for (int l = 0; l < p.N_colloids; ++l) {
+        centres.push_back(hb.coll_x[l]);
+        centres.push_back(hb.coll_y[l]);
+        centres.push_back(hb.coll_z[l]);
+      }
+      B.wall_width = p.wall_width;
+      B.R2 = p.coll_R * p.coll_R;
+      B.mass = hb.lattice_m;
+      B.y_bottom = p.y_bottom;
+      B.y_top = p.y_top;
+      ib_of_box[b] = (int)ib.size();
+      ib.push_back(B);
+    }
+  }
+  if (!ib.empty()) {
+    const int nblk = (int)blk_box.size();
+    std::vector<int> counts(3 * (size_t)nblk);
+    int* d_counts = nullptr;
+    bool ok = tmp.alloc(&d_ib, ib.size()) && tmp.alloc(&d_blk_box, nblk) &&
+              tmp.alloc(&d_centres, std::max<size_t>(centres.size(), 1)) &&
+              tmp.alloc(&d_counts, counts.size());
+    ok = ok && cudaMemcpyAsync(d_ib, ib.data(), ib.size() * sizeof(InitBox),
+                               cudaMemcpyHostToDevice, c->stream) == cudaSuccess;
+    ok = ok && cudaMemcpyAsync(d_blk_box, blk_box.data(), nblk * sizeof(int),
+                               cudaMemcpyHostToDevice, c->stream) == cudaSuccess;
+    ok = ok && (centres.empty() ||
+                cudaMemcpyAsync(d_centres, centres.data(), centres.size() * sizeof(double),
+                                cudaMemcpyHostToDevice, c->stream) == cudaSuccess);
+    ok = ok && launch_init_count(d_ib, d_blk_box, nblk, d_centres, d_counts, c->stream) == 0;
+    ok = ok && cudaMemcpyAsync(counts.data(), d_counts, counts.size() * sizeof(int),
+                               cudaMemcpyDeviceToHost, c->stream) == cudaSuccess;
+    ok = ok && cudaStreamSynchronize(c->stream) == cudaSuccess;
+    if (!ok) {
+      fprintf(stderr, "sph_create: device initialisation failed\n");
+      free_ctx(c);
+      return SPH_ERR_CUDA;
+    }
+    // per-block offsets within each box, and the boxes' particle and wall counts
+    offs.assign(counts.size(), 0);
+    for (InitBox& B : ib) {
+      int n[3] = {0, 0, 0};
+      for (int k = B.blk0; k < B.blk0 + B.nblk; ++k)
+        for (int q = 0; q < 3; ++q) {
+          offs[3 * (size_t)k + q] = n[q];
+          n[q] += counts[3 * (size_t)k + q];
+        }
+      HostBox& hb = c->boxes[B.box];
+      hb.host0 = n[0];
+      hb.p.N = n[0] + (int)hb.x.size();
+      if (hb.p.N > hb.Nmax) {
+        fprintf(stderr, "sph_create: box %d: N > Nmax while building colloid shells\n", B.box);
+        free_ctx(c);
+        return SPH_ERR_BAD_INPUT;
+      }
+      if (hb.p.wall) {
+        hb.walls_start[0] = 0;
+        hb.walls_start[1] = n[1];
+        hb.Nlist_walls = n[1] + n[2];
+      }
+      B.nw1 = n[1];
+    }
+  }
   // ---- offsets ----
   int Ntot = 0, Ctot = 0, ncoll = 0, nwall = 0, ncc = 0, nlist = 0, nwl = 0;
   for (HostBox& hb : c->boxes) {
@@ -429,7 +535,7 @@ sph_status sph_create_ensemble(int nboxes, const sph_input* inputs,
     nwall += p.wall ? 2 : 0;
     ncc += p.N_colloids > 0 ? p.Ntotal_cells_colloids : 0;
     nlist += (int)hb.colloids_list.size();
-    nwl += (int)hb.walls_list.size();
+    nwl += p.wall ? hb.Nlist_walls : 0;
     c->max_coll = std::max(c->max_coll, p.N_colloids);
   }
   Dev& d = c->d;
@@ -500,30 +606,52 @@ sph_status sph_create_ensemble(int nboxes, const sph_input* inputs,
     return SPH_ERR_NOMEM;
   }
   // ---- host images in id order (slot = id at start) ----
-  std::vector<double4> pos(Np), vel(Np);
-  std::vector<double> conf(6 * Np, 0.0);
-  std::vector<int> tinfo(Np, 0), gid(Np, 0), cell_box(Ctot), wl, wseg{0}, cl, cseg{0}, cbox;
+  // Without device initialisation the whole state is imaged on the host.  With it, only
+  // the host-built particles (colloid shells, restart boxes) are packed and scattered.
+  const bool full = !dev_init;
+  size_t nh = 0;
+  for (const HostBox& hb : c->boxes) nh += hb.x.size();
+  std::vector<double4> pos(full ? Np : 0), vel(full ? Np : 0), hpos, hvel;
+  std::vector<double> conf(full ? 6 * Np : 0, 0.0), hconf(full ? 0 : 6 * nh);
+  std::vector<int2> hmeta;
+  std::vector<int> tinfo(full ? Np : 0, 0), gid(full ? Np : 0, 0), cell_box(Ctot), wl,
+      wseg{0}, cl, cseg{0}, cbox;
   std::vector<double> xc(3 * (size_t)std::max(nlist, 1), 0.0), cs((size_t)kCollFields * std::max(ncoll, 1), 0.0);
   std::vector<BoxParams> params;
   for (int b = 0; b < nboxes; ++b) {
     const HostBox& hb = c->boxes[b];
     const BoxParams& p = hb.p;
     params.push_back(p);
-    for (int i = 0; i < p.N; ++i) {
-      const int s = p.slot0 + i;
-      pos[s] = make_double4(hb.x[i], hb.y[i], hb.z[i], hb.mass[i]);
-      vel[s] = make_double4(hb.vx[i], hb.vy[i], hb.vz[i], 0.0);
-      conf[0 * Np + s] = hb.cxx[i];
-      conf[1 * Np + s] = hb.cxy[i];
-      conf[2 * Np + s] = hb.cyy[i];
-      conf[3 * Np + s] = hb.cxz[i];
-      conf[4 * Np + s] = hb.cyz[i];
-      conf[5 * Np + s] = hb.czz[i];
-      tinfo[s] = (hb.type[i] & kTypeMask) | (b << kTypeBits);
-      gid[s] = s;
+    for (int i = 0; i < (int)hb.x.size(); ++i) {
+      const int s = p.slot0 + hb.host0 + i;
+      const double4 x4 = make_double4(hb.x[i], hb.y[i], hb.z[i], hb.mass[i]);
+      const double4 v4 = make_double4(hb.vx[i], hb.vy[i], hb.vz[i], 0.0);
+      const double c6[6] = {hb.cxx[i], hb.cxy[i], hb.cyy[i], hb.cxz[i], hb.cyz[i], hb.czz[i]};
+      const int t = (hb.type[i] & kTypeMask) | (b << kTypeBits);
+      if (full) {
+        pos[s] = x4;
+        vel[s] = v4;
+        for (int q = 0; q < 6; ++q) conf[q * Np + s] = c6[q];
+        tinfo[s] = t;
+        gid[s] = s;
+      } else {
+        const size_t k = hmeta.size();
+        hmeta.push_back(make_int2(s, t));
+        hpos.push_back(x4);
+        hvel.push_back(v4);
+        for (int q = 0; q < 6; ++q) hconf[q * nh + k] = c6[q];
+      }
     }
     for (int q = 0; q < p.Ntotal_cells; ++q) cell_box[p.cell0 + q] = b;
-    if (p.wall) {
+    if (p.wall && hb.lattice_on_device) {
+      // entries written by the fill pass
+      InitBox& B = ib[ib_of_box[b]];
+      B.slot0 = p.slot0;
+      B.wl0 = (int)wl.size();
+      wl.resize(wl.size() + hb.Nlist_walls, -1);
+      wseg.push_back(B.wl0 + hb.walls_start[1]);
+      wseg.push_back((int)wl.size());
+    } else if (p.wall) {
       const int w1 = hb.walls_start[1];
       for (int k = 0; k < (int)hb.walls_list.size(); ++k) {
         if (k == w1) wseg.push_back((int)wl.size());
@@ -538,7 +666,7 @@ sph_status sph_create_ensemble(int nboxes, const sph_input* inputs,
       const int k1 = k + 1 < p.N_colloids ? hb.colloids_start[k + 1] : (int)hb.colloids_list.size();
       for (int q = k0; q < k1; ++q) {
         const int e = (int)cl.size();
-        cl.push_back(p.slot0 + hb.colloids_list[q]);
+        cl.push_back(p.slot0 + hb.host0 + hb.colloids_list[q]);
         xc[e] = hb.x_center[q];
         xc[(size_t)std::max(nlist, 1) + e] = hb.y_center[q];
         xc[2 * (size_t)std::max(nlist, 1) + e] = hb.z_center[q];
@@ -557,12 +685,14 @@ sph_status sph_create_ensemble(int nboxes, const sph_input* inputs,
       ok = false;
   };
   up((void*)d.box, params.data(), params.size() * sizeof(BoxParams));
-  up(d.pos, pos.data(), Np * sizeof(double4));
-  up(d.vel, vel.data(), Np * sizeof(double4));
-  up(d.conf, conf.data(), conf.size() * sizeof(double));
-  up(d.tinfo, tinfo.data(), Np * sizeof(int));
-  up(d.gid, gid.data(), Np * sizeof(int));
-  up(d.inv, gid.data(), Np * sizeof(int));
+  if (full) {
+    up(d.pos, pos.data(), Np * sizeof(double4));
+    up(d.vel, vel.data(), Np * sizeof(double4));
+    up(d.conf, conf.data(), conf.size() * sizeof(double));
+    up(d.tinfo, tinfo.data(), Np * sizeof(int));
+    up(d.gid, gid.data(), Np * sizeof(int));
+    up(d.inv, gid.data(), Np * sizeof(int));
+  }
   up(d.cell_box, cell_box.data(), cell_box.size() * sizeof(int));
   up(d.walls_list, wl.data(), wl.size() * sizeof(int));
   up(d.wall_seg, wseg.data(), wseg.size() * sizeof(int));
@@ -573,6 +703,29 @@ sph_status sph_create_ensemble(int nboxes, const sph_input* inputs,
   up(d.cs, cs.data(), cs.size() * sizeof(double));
   up(d.ke_chunk, kchunk.data(), kchunk.size() * sizeof(int));
   up(d.ke_box_chunk, kbox.data(), kbox.size() * sizeof(int));
+  if (ok && !full) {
+    // the lattice boxes' particles and walls lists, then the host-built particles
+    const Launch L = launcher(c);
+    if (!ib.empty()) {
+      int* d_offs = nullptr;
+      ok = tmp.alloc(&d_offs, offs.size());
+      up(d_ib, ib.data(), ib.size() * sizeof(InitBox));
+      up(d_offs, offs.data(), offs.size() * sizeof(int));
+      ok = ok && launch_init_fill(L, d_ib, d_blk_box, (int)blk_box.size(), d_centres, d_offs) == 0;
+    }
+    if (ok && nh > 0) {
+      int2* d_meta = nullptr;
+      double4 *d_hpos = nullptr, *d_hvel = nullptr;
+      double* d_hconf = nullptr;
+      ok = tmp.alloc(&d_meta, nh) && tmp.alloc(&d_hpos, nh) && tmp.alloc(&d_hvel, nh) &&
+           tmp.alloc(&d_hconf, 6 * nh);
+      up(d_meta, hmeta.data(), nh * sizeof(int2));
+      up(d_hpos, hpos.data(), nh * sizeof(double4));
+      up(d_hvel, hvel.data(), nh * sizeof(double4));
+      up(d_hconf, hconf.data(), 6 * nh * sizeof(double));
+      ok = ok && launch_init_scatter(L, (int)nh, d_meta, d_hpos, d_hvel, d_hconf) == 0;
+    }
+  }
   if (!ok || cudaStreamSynchronize(c->stream) != cudaSuccess) {
     fprintf(stderr, "sph_create: upload failed: %s\n", cudaGetErrorString(cudaGetLastError()));
     free_ctx(c);

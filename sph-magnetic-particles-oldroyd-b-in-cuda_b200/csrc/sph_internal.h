@@ -68,6 +68,13 @@ struct HostBox {
   std::vector<double> x_center, y_center, z_center;
   std::vector<double> coll_x, coll_y, coll_z;
   int Nmax = 0;  // reserved particles (system_constructor.cpp:62-79)
+  // Lattice generated on the device (sph_init.cu): the host arrays above then hold only
+  // the colloid shells, which follow the nlat lattice particles in the box's id order.
+  bool lattice_on_device = false;
+  int Nxyz[3] = {0, 0, 0};  // lattice sites per direction, wall rows included
+  double dx[3] = {0.0, 0.0, 0.0};
+  double lattice_m = 0.0;   // particle mass of the lattice
+  int host0 = 0;            // box-local id of the first host-built particle (= nlat)
 };
 
 // Scalar summary of a box (sph_info), step / nboxes / precision left zero.
@@ -77,8 +84,10 @@ void fill_info(const HostBox& hb, sph_info* o);
 sph_status parse_input_file(const char* path, sph_input* in, std::vector<double>* coll,
                             std::string* msg);
 // Builds a box from its inputs (constructor + initialize of the reference).
+// With lattice_on_device, a lattice box (new_sim 0) gets its parameters and colloid shells
+// only; its lattice, walls list and particle count come from the device (sph_init.cu).
 sph_status build_box(const sph_input& in, const char* particles_path, HostBox* box,
-                     std::string* msg);
+                     std::string* msg, bool lattice_on_device = false);
 
 // Neighbour-record layouts (one per particle, slot order), written by the density
 // epilogue and gathered by the pair kernel.  P holds Pi/d^2 = (p I - nkT c)/d^2 for
@@ -211,6 +220,30 @@ int launch_observe(const Launch& L, double* ke_partial, double* obs_partial, dou
 int launch_gather_field(const Launch& L, int field, double* out);
 int launch_scatter_field(const Launch& L, int field, const double* in);
 int launch_gather_int(const Launch& L, const int* src, int* out);
+
+// Device-side initialisation of a lattice box (sph_init.cu).  Sites are processed in
+// blocks of kInitThreads; a box owns the blocks [blk0, blk0 + nblk).
+constexpr int kInitThreads = 256;
+struct InitBox {
+  int box;          // box index (type word)
+  int dim, wall;
+  int Nxyz[3];      // lattice sites per direction, wall rows included
+  int nsites;       // Nxyz product (Nxyz[2] taken as 1 in 2D)
+  int blk0, nblk;
+  int coll0, ncoll; // the box's colloid centres in the centres array (3 doubles each)
+  int slot0;        // fill pass: first slot of the box
+  int wl0, nw1;     // fill pass: first walls_list entry, bottom-wall particles
+  double dx[3], wall_width, R2, mass, L[3], y_bottom, y_top;
+};
+// counts: 3 per block (kept, bottom wall, top wall)
+int launch_init_count(const InitBox* boxes, const int* blk_box, int nblk, const double* centres,
+                      int* counts, void* stream);
+// offs: 3 per block, the box-local counts before the block
+int launch_init_fill(const Launch& L, const InitBox* boxes, const int* blk_box, int nblk,
+                     const double* centres, const int* offs);
+// host-built particles, packed: (slot, type word), position + mass, velocity, conformation
+int launch_init_scatter(const Launch& L, int n, const int2* meta, const double4* pos,
+                        const double4* vel, const double* conf);
 
 // Stable LSD radix sort of the hash keys (sph_sort.cu): keys d.key_by_gid indexed by
 // global id, values = global ids; result in d.keys / d.vals.

@@ -8,7 +8,8 @@
 // writer thread; the GPU goes on with the next steps while the files are formatted.
 //
 //   sph_run [--input FILE] [--particles FILE] [--precision fp64|mixed] [--no-graph]
-//           [--steps N] [--checkpoint FILE] [--restart FILE] [--autotune CACHE] [--quiet]
+//           [--steps N] [--checkpoint FILE] [--restart FILE] [--autotune CACHE]
+//           [--device-init] [--quiet]
 #include <chrono>
 #include <condition_variable>
 #include <cstdio>
@@ -34,6 +35,7 @@ struct Args {
   int steps = -1;  // -1: Nsteps of the input file
   std::string checkpoint, restart, autotune;
   bool quiet = false;
+  bool device_init = false;
 };
 
 bool parse_args(int argc, char** argv, Args* a) {
@@ -65,6 +67,8 @@ bool parse_args(int argc, char** argv, Args* a) {
       if (!next(&a->restart)) return false;
     } else if (s == "--autotune") {
       if (!next(&a->autotune)) return false;
+    } else if (s == "--device-init") {
+      a->device_init = true;
     } else if (s == "--quiet") {
       a->quiet = true;
     } else {
@@ -178,7 +182,7 @@ int main(int argc, char** argv) {
     std::fprintf(stderr,
                  "usage: sph_run [--input FILE] [--particles FILE] [--precision fp64|mixed]\n"
                  "               [--no-graph] [--steps N] [--checkpoint FILE] [--restart FILE]"
-                 " [--autotune CACHE] [--quiet]\n");
+                 " [--autotune CACHE] [--device-init] [--quiet]\n");
     return 2;
   }
   sph_input in;
@@ -194,6 +198,7 @@ int main(int argc, char** argv) {
   std::memset(&opt, 0, sizeof(opt));
   opt.precision = a.precision;
   opt.use_graph = a.graph ? 1 : 0;
+  opt.init_on_device = a.device_init ? 1 : 0;
   sph_ctx* ctx = nullptr;
   s = sph_create(&in, a.particles.empty() ? nullptr : a.particles.c_str(), &opt, &ctx);
   if (s != SPH_OK) return fail("create", s, nullptr);

@@ -12,6 +12,8 @@
 #include <string>
 #include <vector>
 
+#include <climits>
+
 #include "sph_internal.h"
 
 namespace sph {
@@ -211,6 +213,17 @@ sph_status validate(const sph_input& in, std::string* msg) {
   return SPH_OK;
 }
 
+// Particle mass of the lattice (system_initialize_particles_new_sim.cpp:127-131).
+double lattice_mass(const HostBox& hb, const int Nxyz[3]) {
+  const BoxParams& p = hb.p;
+  if (p.dim == 2)
+    return hb.in.rho * p.L[0] * (p.L[1] + 2.0 * p.wall_width) / (Nxyz[0] * Nxyz[1]);
+  return hb.in.rho * p.L[0] * (p.L[1] + 2.0 * p.wall_width) * p.L[2] /
+         (Nxyz[0] * Nxyz[1] * Nxyz[2]);
+}
+
+sph_status colloid_shells(HostBox* hb, const double dx[3], int Nmax, std::string* msg);
+
 // Lattice + colloid shells (system_initialize_particles_new_sim.cpp:16-253).
 sph_status lattice_particles(HostBox* hb, const int Nxyz[3], const double dx[3], int Nmax,
                              std::string* msg) {
@@ -248,21 +261,23 @@ sph_status lattice_particles(HostBox* hb, const int Nxyz[3], const double dx[3],
   if (p.wall)
     for (size_t i = 0; i < nfluid; ++i)
       hb->type[i] = hb->y[i] < p.y_bottom ? 1 : (hb->y[i] > p.y_top ? 2 : 0);
-  double m;
-  if (dim == 2)
-    m = hb->in.rho * p.L[0] * (p.L[1] + 2.0 * p.wall_width) / (Nxyz[0] * Nxyz[1]);
-  else
-    m = hb->in.rho * p.L[0] * (p.L[1] + 2.0 * p.wall_width) * p.L[2] /
-        (Nxyz[0] * Nxyz[1] * Nxyz[2]);
-  hb->mass.assign(nfluid, m);
+  hb->mass.assign(nfluid, lattice_mass(*hb, Nxyz));
   hb->cxx.assign(nfluid, 1.0);
   hb->cyy.assign(nfluid, 1.0);
   hb->czz.assign(nfluid, 1.0);
   hb->cxy.assign(nfluid, 0.0);
   hb->cxz.assign(nfluid, 0.0);
   hb->cyz.assign(nfluid, 0.0);
-  // Colloid shells.  Shell particles get no velocity, mass or conformation values in the
-  // reference (it fills those for lattice particles only); they are zero here.
+  return colloid_shells(hb, dx, Nmax, msg);
+}
+
+// Colloid shells (system_initialize_particles_new_sim.cpp:142-249), appended after the
+// particles already in hb.  Shell particles get no velocity, mass or conformation values
+// in the reference (it fills those for lattice particles only); they are zero here.
+// Fails once the box would exceed Nmax particles.
+sph_status colloid_shells(HostBox* hb, const double dx[3], int Nmax, std::string* msg) {
+  BoxParams& p = hb->p;
+  const int dim = p.dim;
   auto add = [&](double px, double py, double pz, int t) -> bool {
     if ((int)hb->x.size() + 1 > Nmax) return false;
     hb->x.push_back(px);
@@ -381,7 +396,7 @@ sph_status restart_particles(HostBox* hb, const char* path, std::string* msg) {
 // class_system::constructor + initialize (system_constructor.cpp:15-108,
 // system_initialize.cpp:16-359)
 sph_status build_box(const sph_input& in_, const char* particles_path, HostBox* hb,
-                     std::string* msg) {
+                     std::string* msg, bool lattice_on_device) {
   sph_status st = validate(in_, msg);
   if (st != SPH_OK) return st;
   hb->in = in_;
@@ -508,7 +523,22 @@ sph_status build_box(const sph_input& in_, const char* particles_path, HostBox* 
     int Nmax = dim == 2 ? Nxyz[0] * Ny_ctor : Nxyz[0] * Ny_ctor * Nxyz[2];
     if (nc > 0) Nmax = (int)(Nmax * 1.01);
     hb->Nmax = Nmax;
-    st = lattice_particles(hb, Nxyz, dx, Nmax, msg);
+    if (lattice_on_device) {
+      // the lattice is generated on the device (sph_init.cu); the host keeps the shells,
+      // whose Nmax check waits for the device's count of lattice particles
+      hb->lattice_on_device = true;
+      for (int q = 0; q < 3; ++q) {
+        hb->Nxyz[q] = Nxyz[q];
+        hb->dx[q] = dx[q];
+      }
+      hb->lattice_m = lattice_mass(*hb, Nxyz);
+      hb->x.clear(); hb->y.clear(); hb->z.clear(); hb->type.clear(); hb->mass.clear();
+      hb->cxx.clear(); hb->cxy.clear(); hb->cyy.clear();
+      hb->cxz.clear(); hb->cyz.clear(); hb->czz.clear();
+      st = colloid_shells(hb, dx, INT_MAX, msg);
+    } else {
+      st = lattice_particles(hb, Nxyz, dx, Nmax, msg);
+    }
   } else {
     st = restart_particles(hb, particles_path, msg);
   }
@@ -596,7 +626,7 @@ void fill_info(const HostBox& hb, sph_info* o) {
   }
   o->Ntotal_cells = p.Ntotal_cells;
   o->Nwalls = p.wall ? 2 : 0;
-  o->Nlist_walls = (int)hb.walls_list.size();
+  o->Nlist_walls = hb.Nlist_walls;
   o->N_colloids = p.N_colloids;
   o->Nlist_colloids = (int)hb.colloids_list.size();
   o->Ntotal_cells_colloids = p.Ntotal_cells_colloids;
