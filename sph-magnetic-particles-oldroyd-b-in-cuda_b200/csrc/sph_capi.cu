@@ -643,10 +643,10 @@ sph_status sph_create_ensemble(int nboxes, const sph_input* inputs,
       }
     }
     for (int q = 0; q < p.Ntotal_cells; ++q) cell_box[p.cell0 + q] = b;
+    if (hb.lattice_on_device) ib[ib_of_box[b]].slot0 = p.slot0;
     if (p.wall && hb.lattice_on_device) {
       // entries written by the fill pass
       InitBox& B = ib[ib_of_box[b]];
-      B.slot0 = p.slot0;
       B.wl0 = (int)wl.size();
       wl.resize(wl.size() + hb.Nlist_walls, -1);
       wseg.push_back(B.wl0 + hb.walls_start[1]);

@@ -69,6 +69,38 @@ def test_device_init_ensemble_matches_host(precision, workdir):
     host.close()
 
 
+def test_device_init_mixed_walled_and_periodic(workdir):
+    """Walled and periodic boxes, with and without colloids, in one context: each lattice
+    box lands at its own slots and walls-list entries."""
+    import sph_input
+
+    specs = [
+        dict(N=(32, 32), L=(1.0, 1.0), dim=2, overlap=4.0, wall=1, Vwall_top=0.3,
+             Vwall_bottom=-0.3, dt=2e-5),
+        dict(N=(40, 40), L=(1.0, 1.0), dim=2, overlap=4.0, wall=0, ext_force_type=2,
+             ext_force=(1.0, 0.0), dt=5e-5),
+        dict(N=(48, 40), L=(1.2, 1.0), dim=2, overlap=4.0, wall=1, Vwall_top=0.1,
+             Vwall_bottom=-0.1, dt=2e-5, tau=2.0, N_colloids=2, coll_R=4.0 / 40,
+             coll_x=((0.3, 0.5), (0.8, 0.45)), tau_repulsion=5.0, cutoff_magnetic=0.3,
+             F0_magnetic=1e-4, F0_repulsion=1e-3, omega_magnetic=3.0),
+        dict(N=(36, 36), L=(1.0, 1.0), dim=2, overlap=4.0, wall=0, dt=2e-5, N_colloids=1,
+             coll_R=4.0 / 36, coll_x=((0.97, 0.03),), tau_repulsion=5.0, cutoff_magnetic=0.3,
+             F0_magnetic=1e-4, F0_repulsion=1e-3, omega_magnetic=3.0),
+        dict(N=(32, 32), L=(1.0, 1.0), dim=2, overlap=3.0, wall=1, Vwall_top=0.5,
+             Vwall_bottom=-0.5, dt=2e-5),
+    ]
+    paths = []
+    for k, spec in enumerate(specs):
+        p = os.path.join(workdir, "input%d" % k)
+        sph_input.write_input(p, **spec)
+        paths.append(p)
+    host = sph_b200.System(paths, init_on_device=False)
+    dev = sph_b200.System(paths, init_on_device=True)
+    assert_same(dev, host, "walled+periodic", steps=3)
+    dev.close()
+    host.close()
+
+
 def test_device_init_periodic_colloids_3d(workdir):
     """Colloids near the periodic faces of a walled 3D box: the carving wraps in x and z
     (and not in y, where the walls are)."""
