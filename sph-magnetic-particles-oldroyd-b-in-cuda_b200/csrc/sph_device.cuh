@@ -338,16 +338,50 @@ struct PairOwn {
   bool fluid, do_grad, do_force;
 };
 
+// Compensated summation of the float pair sums (density, velocity gradient, forces) in
+// mixed precision; FP64 sums stay plain.
+#ifndef SPH_FLOAT_SUMS_COMPENSATED
+#define SPH_FLOAT_SUMS_COMPENSATED 1
+#endif
+template <typename T>
+struct Compensated {
+  static constexpr bool on = false;
+};
+template <>
+struct Compensated<float> {
+  static constexpr bool on = SPH_FLOAT_SUMS_COMPENSATED != 0;
+};
+
+// Kahan step: s + c tracks the exact sum of the terms to about one rounding of s.
+__device__ __forceinline__ void kahan_add(float& s, float& c, float x) {
+  const float y = __fsub_rn(x, c);
+  const float t = __fadd_rn(s, y);
+  c = __fsub_rn(__fsub_rn(t, s), y);
+  s = t;
+}
+
 template <typename T, int DIM>
 struct PairAcc {
+  // float sums (mixed precision) are compensated: each carries its rounding error in a
+  // second float (Kahan), added back when the sum is stored
+  static constexpr bool kComp = Compensated<T>::on;
   T g[DIM][DIM];
   T f[3];
+  T cg[DIM][DIM];
+  T cf[3];
   __device__ __forceinline__ void zero() {
 #pragma unroll
     for (int a = 0; a < DIM; ++a)
 #pragma unroll
-      for (int c = 0; c < DIM; ++c) g[a][c] = T(0);
+      for (int c = 0; c < DIM; ++c) g[a][c] = cg[a][c] = T(0);
     f[0] = f[1] = f[2] = T(0);
+    cf[0] = cf[1] = cf[2] = T(0);
+  }
+  __device__ __forceinline__ double grad(int a, int c) const {
+    return kComp ? (double)g[a][c] - (double)cg[a][c] : (double)g[a][c];
+  }
+  __device__ __forceinline__ double force(int a) const {
+    return kComp ? (double)f[a] - (double)cf[a] : (double)f[a];
   }
 };
 
@@ -406,7 +440,12 @@ __device__ __forceinline__ void pair_term(const BoxParams& p, const PairParams<T
     for (int a = 0; a < DIM; ++a) {
       const T se = s * e[a];
 #pragma unroll
-      for (int c = 0; c < DIM; ++c) acc.g[a][c] += se * v[c];
+      for (int c = 0; c < DIM; ++c) {
+        if constexpr (PairAcc<T, DIM>::kComp)
+          kahan_add(acc.g[a][c], acc.cg[a][c], se * v[c]);
+        else
+          acc.g[a][c] += se * v[c];
+      }
     }
   }
   if (pair_force) {
@@ -445,7 +484,24 @@ __device__ __forceinline__ void pair_term(const BoxParams& p, const PairParams<T
     const T ayy = -gw * (Pi[2] + Pj[2]);
     const T aux = gw * di * dj * rinv;
     const T aux1 = pp.a * aux;
-    if (DIM == 2) {
+    if constexpr (PairAcc<T, DIM>::kComp) {
+      // the pair's force as one term per component, then one compensated add
+      T ev = e[0] * v[0] + e[1] * v[1];
+      T t0 = axx * e[0] + axy * e[1], t1 = axy * e[0] + ayy * e[1], t2 = T(0);
+      if (DIM == 3) {
+        const T axz = -gw * (Pi[3] + Pj[3]);
+        const T ayz = -gw * (Pi[4] + Pj[4]);
+        const T azz = -gw * (Pi[5] + Pj[5]);
+        ev += e[2] * v[2];
+        t0 += axz * e[2];
+        t1 += ayz * e[2];
+        t2 = axz * e[0] + ayz * e[1] + azz * e[2];
+      }
+      const T aux2 = pp.b * aux * ev;
+      kahan_add(acc.f[0], acc.cf[0], t0 + (aux1 * v[0] + aux2 * e[0]));
+      kahan_add(acc.f[1], acc.cf[1], t1 + (aux1 * v[1] + aux2 * e[1]));
+      if (DIM == 3) kahan_add(acc.f[2], acc.cf[2], t2 + (aux1 * v[2] + aux2 * e[2]));
+    } else if (DIM == 2) {
       const T ev = e[0] * v[0] + e[1] * v[1];
       acc.f[0] += axx * e[0] + axy * e[1];
       acc.f[1] += axy * e[0] + ayy * e[1];
@@ -476,20 +532,20 @@ __device__ __forceinline__ void pair_store(const Dev& d, int i, const BoxParams&
   const int Np2 = d.Npad;
   if (MODE == kPairGradvAll || (MODE == kPairFused && d.gradv != nullptr && o.do_grad)) {
     // storage order xx xy xz yx yy yz zx zy zz
-    d.gradv[0 * Np2 + i] = (double)acc.g[0][0];
-    d.gradv[1 * Np2 + i] = (double)acc.g[0][1];
-    d.gradv[3 * Np2 + i] = (double)acc.g[1][0];
-    d.gradv[4 * Np2 + i] = (double)acc.g[1][1];
+    d.gradv[0 * Np2 + i] = acc.grad(0, 0);
+    d.gradv[1 * Np2 + i] = acc.grad(0, 1);
+    d.gradv[3 * Np2 + i] = acc.grad(1, 0);
+    d.gradv[4 * Np2 + i] = acc.grad(1, 1);
     if (DIM == 3) {
-      d.gradv[2 * Np2 + i] = (double)acc.g[0][DIM - 1];
-      d.gradv[5 * Np2 + i] = (double)acc.g[1][DIM - 1];
-      d.gradv[6 * Np2 + i] = (double)acc.g[DIM - 1][0];
-      d.gradv[7 * Np2 + i] = (double)acc.g[DIM - 1][1];
-      d.gradv[8 * Np2 + i] = (double)acc.g[DIM - 1][DIM - 1];
+      d.gradv[2 * Np2 + i] = acc.grad(0, DIM - 1);
+      d.gradv[5 * Np2 + i] = acc.grad(1, DIM - 1);
+      d.gradv[6 * Np2 + i] = acc.grad(DIM - 1, 0);
+      d.gradv[7 * Np2 + i] = acc.grad(DIM - 1, 1);
+      d.gradv[8 * Np2 + i] = acc.grad(DIM - 1, DIM - 1);
     }
   }
   if (MODE == kPairGradvAll) return;
-  double fx = (double)acc.f[0], fy = (double)acc.f[1], fz = (double)acc.f[2];
+  double fx = acc.force(0), fy = acc.force(1), fz = acc.force(2);
   if (EXT && o.fluid) {
     const double4 xd = d.pos[i];
     const double m = xd.w;
@@ -520,7 +576,8 @@ __device__ __forceinline__ void pair_store(const Dev& d, int i, const BoxParams&
     const double tinv = 1.0 / p.tau;
     const double cxx = d.conf[i], cxy = d.conf[Np2 + i], cyy = d.conf[2 * Np2 + i];
     if (DIM == 2) {
-      const double gxx = acc.g[0][0], gxy = acc.g[0][1], gyx = acc.g[1][0], gyy = acc.g[1][1];
+      const double gxx = acc.grad(0, 0), gxy = acc.grad(0, 1), gyx = acc.grad(1, 0),
+                   gyy = acc.grad(1, 1);
       const double Axx = cxx * gxx + cxy * gyx, Axy = cxx * gxy + cxy * gyy;
       const double Ayx = cxy * gxx + cyy * gyx, Ayy = cxy * gxy + cyy * gyy;
       d.dcdt[i] = 2.0 * Axx + tinv * (1.0 - cxx);
@@ -532,9 +589,10 @@ __device__ __forceinline__ void pair_store(const Dev& d, int i, const BoxParams&
       d.dcdt[5 * Np2 + i] = 0.0;
     } else {
       const double cxz = d.conf[3 * Np2 + i], cyz = d.conf[4 * Np2 + i], czz = d.conf[5 * Np2 + i];
-      const double gxx = acc.g[0][0], gxy = acc.g[0][1], gxz = acc.g[0][DIM - 1];
-      const double gyx = acc.g[1][0], gyy = acc.g[1][1], gyz = acc.g[1][DIM - 1];
-      const double gzx = acc.g[DIM - 1][0], gzy = acc.g[DIM - 1][1], gzz = acc.g[DIM - 1][DIM - 1];
+      const double gxx = acc.grad(0, 0), gxy = acc.grad(0, 1), gxz = acc.grad(0, DIM - 1);
+      const double gyx = acc.grad(1, 0), gyy = acc.grad(1, 1), gyz = acc.grad(1, DIM - 1);
+      const double gzx = acc.grad(DIM - 1, 0), gzy = acc.grad(DIM - 1, 1),
+                   gzz = acc.grad(DIM - 1, DIM - 1);
       const double Axx = cxx * gxx + cxy * gyx + cxz * gzx;
       const double Axy = cxx * gxy + cxy * gyy + cxz * gzy;
       const double Axz = cxx * gxz + cxy * gyz + cxz * gzz;

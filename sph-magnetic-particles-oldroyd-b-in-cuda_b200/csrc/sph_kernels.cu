@@ -637,7 +637,7 @@ __global__ void k_density(Dev d) {
   const int n = min(d.nbr_cnt[i], d.cap);
   // the particle's list row, read four indices at a time one batch ahead
   const int4* __restrict__ row = reinterpret_cast<const int4*>(d.nbr + (size_t)i * d.cap);
-  T dens = T(0);
+  T dens = T(0), comp = T(0);  // comp: Kahan compensation of a float sum
   int4 nxt = n > 0 ? __ldg(&row[0]) : make_int4(0, 0, 0, 0);
   for (int k0 = 0; k0 < n; k0 += 4) {
     const int4 cur = nxt;
@@ -647,10 +647,14 @@ __global__ void k_density(Dev d) {
     for (int q = 0; q < 4; ++q) {
       if (q >= m) break;
       const int j = q == 0 ? cur.x : q == 1 ? cur.y : q == 2 ? cur.z : cur.w;
-      dens = dens + density_term<T, DIM>(xi, P[j], L, h, p.wall, rcutsq, rcut_inv, cw);
+      const T w = density_term<T, DIM>(xi, P[j], L, h, p.wall, rcutsq, rcut_inv, cw);
+      if constexpr (Compensated<T>::on)
+        kahan_add(dens, comp, w);
+      else
+        dens = dens + w;
     }
   }
-  density_epilogue<T>(d, i, p, (double)dens);
+  density_epilogue<T>(d, i, p, (double)dens - (double)comp);
 }
 
 // kernel_pressures.cu:13-23 (standalone, also refreshes the neighbour record)
