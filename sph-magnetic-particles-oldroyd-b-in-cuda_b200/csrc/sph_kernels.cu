@@ -721,8 +721,16 @@ __device__ __forceinline__ void stage_records(int4* buf, const Rec* __restrict__
   }
 }
 
+// Resident blocks per SM the register allocation is held to: 3 (at most 168 registers) for
+// the FP64 3D pass, whose working set spills at 4; 4 for the FP64 2D pass, which fits in
+// 128 registers; the float passes fit 4 blocks either way.
+template <typename T, int DIM>
+constexpr int pair_min_blocks() {
+  return sizeof(T) == 8 && DIM == 2 ? 4 : 3;
+}
+
 template <typename T, int DIM, int MODE, bool EXT>
-__global__ void __launch_bounds__(kPairWarps * 32, 3) k_pairs(Dev d) {
+__global__ void __launch_bounds__(kPairWarps * 32, pair_min_blocks<T, DIM>()) k_pairs(Dev d) {
   using Rec = typename RecOf<T>::type;
   using St = PairStage<Rec>;
   __shared__ int4 stage[kPairWarps][2][32 * St::kStride];
@@ -769,11 +777,17 @@ __global__ void __launch_bounds__(kPairWarps * 32, 3) k_pairs(Dev d) {
     cp_async_wait_prev();  // position k has landed (this lane's copies) ...
     __syncwarp();          // ... and every other lane's
     if (jc >= 0 && jc != i) {
-      typename St::Slot rj;
       const int4* src = sb + (k & 1) * 32 * St::kStride + lane * St::kStride;
+      if constexpr (sizeof(T) == 8) {
+        // FP64: the neighbour's record is read in place, each field loaded where the pair
+        // term uses it, which keeps the 128-byte record out of the register file
+        pair_term<T, DIM>(p, pp, cv, o, *reinterpret_cast<const Rec*>(src), acc);
+      } else {
+        typename St::Slot rj;
 #pragma unroll
-      for (int t = 0; t < St::kPieces; ++t) rj.v[t] = src[t];
-      pair_term<T, DIM>(p, pp, cv, o, rj.r, acc);
+        for (int t = 0; t < St::kPieces; ++t) rj.v[t] = src[t];
+        pair_term<T, DIM>(p, pp, cv, o, rj.r, acc);
+      }
     }
     __syncwarp();  // buffer k & 1 is refilled at position k + 2
     jc = jn;
