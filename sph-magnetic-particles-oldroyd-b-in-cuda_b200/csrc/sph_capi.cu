@@ -520,7 +520,7 @@ sph_status sph_create_ensemble(int nboxes, const sph_input* inputs,
     }
   }
   // ---- offsets ----
-  int Ntot = 0, Ctot = 0, ncoll = 0, nwall = 0, ncc = 0, nlist = 0, nwl = 0;
+  int Ntot = 0, Ctot = 0, ncoll = 0, nwall = 0, ncc = 0, nlist = 0, nwl = 0, nwchunk = 0;
   for (HostBox& hb : c->boxes) {
     BoxParams& p = hb.p;
     p.slot0 = Ntot;
@@ -536,6 +536,10 @@ sph_status sph_create_ensemble(int nboxes, const sph_input* inputs,
     ncc += p.N_colloids > 0 ? p.Ntotal_cells_colloids : 0;
     nlist += (int)hb.colloids_list.size();
     nwl += p.wall ? hb.Nlist_walls : 0;
+    if (p.wall) {
+      const int n1 = hb.walls_start[1], n2 = hb.Nlist_walls - hb.walls_start[1];
+      nwchunk += (n1 + kWallChunk - 1) / kWallChunk + (n2 + kWallChunk - 1) / kWallChunk;
+    }
     c->max_coll = std::max(c->max_coll, p.N_colloids);
   }
   Dev& d = c->d;
@@ -578,6 +582,9 @@ sph_status sph_create_ensemble(int nboxes, const sph_input* inputs,
   ok = ok && dalloc(c, &d.cell_end, Ctot) && dalloc(c, &d.cell_box, Ctot);
   ok = ok && dalloc(c, &d.walls_list, nwl) && dalloc(c, &d.wall_seg, nwall + 1);
   ok = ok && dalloc(c, &d.wall_f, 3 * std::max(nwall, 1));
+  d.nwallchunks = nwchunk;
+  ok = ok && dalloc(c, &d.wall_chunk, nwchunk + 1) && dalloc(c, &d.wall_seg_chunk, nwall + 1);
+  ok = ok && dalloc(c, &d.wall_part, 3 * (size_t)std::max(nwchunk, 1));
   ok = ok && dalloc(c, &d.colloids_list, nlist) && dalloc(c, &d.coll_seg, ncoll + 1);
   ok = ok && dalloc(c, &d.coll_box, ncoll) && dalloc(c, &d.xc, 3 * (size_t)std::max(nlist, 1));
   ok = ok && dalloc(c, &d.cs, (size_t)kCollFields * std::max(ncoll, 1));
@@ -679,7 +686,15 @@ sph_status sph_create_ensemble(int nboxes, const sph_input* inputs,
       cs[CS_Q0 * ncoll + gc] = 1.0;
     }
   }
-  if (Ntot > 0 && (int)tinfo.size() > 0 && nboxes >= (1 << (31 - kTypeBits))) ok = false;
+  // chunks of the walls lists for the wall-force reduction
+  std::vector<int> wchunk{0}, wsegchunk{0};
+  for (size_t sgm = 0; sgm + 1 < wseg.size(); ++sgm) {
+    for (int j = wseg[sgm]; j < wseg[sgm + 1]; j += kWallChunk)
+      wchunk.push_back(std::min(j + kWallChunk, wseg[sgm + 1]));
+    wsegchunk.push_back((int)wchunk.size() - 1);
+  }
+  if ((int)wchunk.size() - 1 != nwchunk || (int)wsegchunk.size() - 1 != nwall) ok = false;
+  if (nboxes >= (1 << (31 - kTypeBits))) ok = false;
   auto up = [&](void* dst, const void* src, size_t bytes) {
     if (bytes && cudaMemcpyAsync(dst, src, bytes, cudaMemcpyHostToDevice, c->stream) != cudaSuccess)
       ok = false;
@@ -696,6 +711,8 @@ sph_status sph_create_ensemble(int nboxes, const sph_input* inputs,
   up(d.cell_box, cell_box.data(), cell_box.size() * sizeof(int));
   up(d.walls_list, wl.data(), wl.size() * sizeof(int));
   up(d.wall_seg, wseg.data(), wseg.size() * sizeof(int));
+  up(d.wall_chunk, wchunk.data(), wchunk.size() * sizeof(int));
+  up(d.wall_seg_chunk, wsegchunk.data(), wsegchunk.size() * sizeof(int));
   up(d.colloids_list, cl.data(), cl.size() * sizeof(int));
   up(d.coll_seg, cseg.data(), cseg.size() * sizeof(int));
   up(d.coll_box, cbox.data(), cbox.size() * sizeof(int));

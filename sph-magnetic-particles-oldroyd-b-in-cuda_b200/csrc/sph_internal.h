@@ -151,6 +151,10 @@ struct Dev {
   int* walls_list;     // global ids
   int* wall_seg;       // nwallseg + 1 segment boundaries into walls_list
   double* wall_f;      // nwallseg x 3
+  int* wall_chunk;     // nwallchunks + 1 boundaries into walls_list, never across segments
+  int* wall_seg_chunk; // nwallseg + 1 boundaries into the chunks
+  double* wall_part;   // nwallchunks x 3 partial sums
+  int nwallchunks;
   // colloids
   int* colloids_list;  // global ids
   int* coll_seg;       // ncoll + 1 segment boundaries into colloids_list
@@ -177,6 +181,9 @@ enum CollField {
   CS_X = 0, CS_Y, CS_Z, CS_VX, CS_VY, CS_VZ, CS_OX, CS_OY, CS_OZ, CS_THETA, CS_Q0, CS_QX,
   CS_QY, CS_QZ, CS_FX, CS_FY, CS_FZ, CS_TX, CS_TY, CS_TZ, kCollFields
 };
+
+// Entries of a walls list summed by one block of the wall-force reduction.
+constexpr int kWallChunk = 512;
 
 // Kernel launchers (sph_kernels.cu); all asynchronous on `stream`.
 struct Launch {

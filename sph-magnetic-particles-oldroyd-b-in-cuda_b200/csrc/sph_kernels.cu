@@ -890,11 +890,12 @@ __device__ __forceinline__ void block_reduce(double (&v)[NV], double (*sh)[kRedT
   for (int q = 0; q < NV; ++q) v[q] = sh[q][0];
 }
 
+// Pass 1: one block per chunk of a wall's list (kWallChunk entries at most).
 __global__ void __launch_bounds__(kRedThreads) k_wall_forces(Dev d) {
   __shared__ double sh[3][kRedThreads];
-  const int w = blockIdx.x;
-  if (w >= d.nwallseg) return;
-  const int j0 = d.wall_seg[w], j1 = d.wall_seg[w + 1];
+  const int k = blockIdx.x;
+  if (k >= d.nwallchunks) return;
+  const int j0 = d.wall_chunk[k], j1 = d.wall_chunk[k + 1];
   const int Np = d.Npad;
   double v[3] = {0.0, 0.0, 0.0};
   for (int j = j0 + threadIdx.x; j < j1; j += kRedThreads) {
@@ -905,6 +906,29 @@ __global__ void __launch_bounds__(kRedThreads) k_wall_forces(Dev d) {
   }
   block_reduce<3>(v, sh);
   if (threadIdx.x == 0) {
+    d.wall_part[3 * k + 0] = v[0];
+    d.wall_part[3 * k + 1] = v[1];
+    d.wall_part[3 * k + 2] = v[2];
+  }
+}
+
+// Pass 2: one warp per wall adds its chunks' partial sums in a fixed order.
+__global__ void k_wall_forces_final(Dev d) {
+  const int w = blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5);
+  const int lane = threadIdx.x & 31;
+  if (w >= d.nwallseg) return;
+  const int c0 = d.wall_seg_chunk[w], c1 = d.wall_seg_chunk[w + 1];
+  double v[3] = {0.0, 0.0, 0.0};
+  for (int c = c0 + lane; c < c1; c += 32) {
+    v[0] += d.wall_part[3 * c + 0];
+    v[1] += d.wall_part[3 * c + 1];
+    v[2] += d.wall_part[3 * c + 2];
+  }
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1)
+#pragma unroll
+    for (int q = 0; q < 3; ++q) v[q] += __shfl_xor_sync(SPH_FULL, v[q], o);
+  if (lane == 0) {
     d.wall_f[3 * w + 0] = v[0];
     d.wall_f[3 * w + 1] = v[1];
     d.wall_f[3 * w + 2] = v[2];
@@ -1381,7 +1405,11 @@ int launch_dcdt_from_gradv(const Launch& L) {
 
 int launch_wall_forces(const Launch& L) {
   if (L.d.nwallseg == 0) return 0;
-  k_wall_forces<<<L.d.nwallseg, kRedThreads, 0, S(L)>>>(L.d);
+  if (L.d.nwallchunks > 0) {
+    k_wall_forces<<<L.d.nwallchunks, kRedThreads, 0, S(L)>>>(L.d);
+    if (check(L)) return 1;
+  }
+  k_wall_forces_final<<<blocks(L.d.nwallseg, 4), 128, 0, S(L)>>>(L.d);
   return check(L);
 }
 
