@@ -241,7 +241,7 @@ def run_ours(args, world, rank, local, dist):
         path = write_workload(wd, args.lattice)
         sysm = sph_b200.System(path, precision=args.precision, device=local)
         n = sysm.N
-        tuning = sysm.autotune()
+        tuning = sysm.autotune() if not args.no_autotune else sysm.tuning()
         sysm.step(args.warmup)
         sysm.synchronize()
         if dist is not None:
@@ -346,7 +346,7 @@ def run_ensemble(args, world, rank, local, dist):
         paths, _ = sph_ensemble.write_inputs([pts[b] for b in mine], wd)
         sysm = sph_b200.System(paths, precision=args.precision, device=local)
         n = sysm.N
-        tuning = sysm.autotune()
+        tuning = sysm.autotune() if not args.no_autotune else sysm.tuning()
         sysm.step(args.warmup)
         sysm.synchronize()
         if dist is not None:
@@ -576,6 +576,8 @@ def main():
                     help="ncu DRAM bytes per k_pairs launch (default: the FP64 capture at "
                          "96^3, 788.8 MB, scaled by particle count to the benchmark)")
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-autotune", action="store_true",
+                    help="keep the default launch geometry (profiling runs: no tuning launches)")
     ap.add_argument("--lattice", type=int, default=128,
                     help="lattice side; 128 is the benchmark, smaller sizes only for ncu captures")
     args = ap.parse_args()

@@ -833,9 +833,12 @@ sph_status sph_calculate_forces(sph_ctx* c, const double* m) {
   Launch L = launcher(c);
   bool ext = false;
   for (const HostBox& hb : c->boxes) ext = ext || hb.p.ext_force_type != 0;
-  // the reference stores the velocity gradient of every particle in this call
-  if (launch_density_dim(L, c->dim) || launch_pairs_dim(L, c->dim, kPairGradvAll, 0) ||
-      launch_pairs_dim(L, c->dim, kPairFused, ext ? 1 : 0) || launch_wall_forces(L))
+  // the reference stores the velocity gradient of every particle in this call: the fused
+  // pass computes it for walls and colloid particles too (same terms, same order as the
+  // standalone gradient pass)
+  L.d.grad_all = 1;
+  if (launch_density_dim(L, c->dim) || launch_pairs_dim(L, c->dim, kPairFused, ext ? 1 : 0) ||
+      launch_wall_forces(L))
     return cuda_fail(c, "calculate_forces");
   bool pairs = false;
   for (const HostBox& hb : c->boxes) pairs = pairs || hb.p.N_colloids >= 2;

@@ -399,8 +399,9 @@ __device__ __forceinline__ void load_own(const Dev& d, int i, const Rec& ri, Pai
   for (int q = 0; q < 6; ++q) o.P[q] = ri.P[q];
   o.t = type_of(ri.tinfo);
   o.fluid = o.t == 0;
-  // gradient: fluid particles in the fused pass, every particle in kPairGradvAll
-  o.do_grad = (MODE == kPairGradvAll) || (MODE == kPairFused && o.fluid);
+  // gradient: every particle in kPairGradvAll; in the fused pass fluid particles (whose
+  // dc/dt needs it), or every particle when the caller stores the whole field
+  o.do_grad = (MODE == kPairGradvAll) || (MODE == kPairFused && (o.fluid || d.grad_all));
   o.do_force = MODE != kPairGradvAll;
 }
 

@@ -174,6 +174,7 @@ struct Dev {
   long long* step;     // device step counter (graph replays)
   unsigned* status;
   int* err_info;       // [0] first bad slot, [1] largest neighbour count seen
+  int grad_all;        // fused pair pass: velocity gradient of every particle, not only fluid
 };
 
 // Colloid state layout in Dev::cs (each row ncoll long).

@@ -179,6 +179,39 @@ def test_class_system_methods_step_by_step(workdir):
     assert ke == pytest.approx(o.kinetic_energy(), rel=1e-12)
 
 
+@pytest.mark.parametrize("name", ["colloids2d", "colloids3d", "couette3d"])
+def test_forces_store_the_same_gradient_as_the_gradient_pass(name, workdir):
+    """calculate_forces stores the velocity gradient of every particle (walls and colloid
+    particles included, kernel_vel_gradients.cu:15-662) from its fused pass: the same bits
+    as the standalone calculate_vel_gradient pass, and the same forces after it."""
+    mg.case_dir(name, workdir)
+    pp = os.path.join(workdir, "input_particles.in")
+    pp = [pp] if os.path.exists(pp) else None
+    e = sph_b200.System(os.path.join(workdir, "input"), pp, use_graph=False)
+    e.step(3)
+    grads = ["gxx", "gxy", "gxz", "gyx", "gyy", "gyz", "gzx", "gzy", "gzz"]
+    if e.info()["dim"] == 2:
+        grads = ["gxx", "gxy", "gyx", "gyy"]
+    m = np.array([0.3, 0.4, 0.0])
+    e.V_Verlet_step1()
+    e.neighbours_search()
+    e.calculate_density()
+    e.calculate_pressure()
+    e.calculate_vel_gradient()
+    g_pass = {f: e.field(f) for f in grads}
+    e.calculate_forces(m)
+    f1 = {f: e.field(f) for f in ["fx", "fy", "fz", "dcdt_xy"]}
+    for f in grads:
+        assert np.array_equal(e.field(f), g_pass[f]), f
+    t = e.type()
+    assert (t != 0).sum() > 0
+    # the same call again: forces and gradient reproduce
+    e.calculate_forces(m)
+    for f, v in f1.items():
+        assert np.array_equal(e.field(f), v), f
+    e.close()
+
+
 def test_device_errors_are_reported_not_trapped(workdir):
     """A non-finite position and a particle outside the wall band come back as statuses;
     the context keeps working once the state is repaired."""
