@@ -313,6 +313,28 @@ __device__ __forceinline__ void ghost_solid_i(const BoxParams& p, const CollView
 // (kernel_forces.cu:15-865), external force (kernel_ext_force.cu:13-73), dc/dt
 // (kernel_dcdt.cu:15-104).  One function for one (i, j) pair, used by every pair kernel.
 // ---------------------------------------------------------------------------------
+// Read-only position loads.  In 3D a double4 is read as one 256-bit access (the vector
+// width of sm_100 global loads): one L1 request per lane instead of two 128-bit ones.  In
+// 2D only x and y are read (one 128-bit access; z and the mass come back zero).  Position
+// arrays are 32-byte aligned (cudaMalloc base, 32-byte elements).
+template <int DIM>
+__device__ __forceinline__ double4 ld_pos(const double4* a) {
+  double4 v;
+  if (DIM == 3) {
+    asm("ld.global.nc.v4.f64 {%0, %1, %2, %3}, [%4];"
+        : "=d"(v.x), "=d"(v.y), "=d"(v.z), "=d"(v.w)
+        : "l"(a));
+  } else {
+    const double2 xy = __ldg(reinterpret_cast<const double2*>(a));
+    v = make_double4(xy.x, xy.y, 0.0, 0.0);
+  }
+  return v;
+}
+template <int DIM>
+__device__ __forceinline__ float4 ld_pos(const float4* a) {
+  return __ldg(a);
+}
+
 template <typename T, int DIM>
 struct PairParams {
   T L[3], h[3], rcutsq, rcut_inv, c_gradw, a, b;

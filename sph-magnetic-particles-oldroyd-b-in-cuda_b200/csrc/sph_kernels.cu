@@ -413,7 +413,7 @@ __global__ void __launch_bounds__(kListWarps * 32) k_build_lists(Dev d) {
     float xi = 0.f, yi = 0.f, zi = 0.f;
     bool odd = false, lost = false;
     if (active) {
-      double4 x = d.pos[i];
+      const double4 x = ld_pos<DIM>(d.pos + i);
       xi = (float)(x.x - ox);
       yi = (float)(x.y - oy);
       zi = (float)(x.z - oz);
@@ -461,7 +461,7 @@ __global__ void __launch_bounds__(kListWarps * 32) k_build_lists(Dev d) {
             const int j = c0 + gl;
             float vx = 1e30f, vy = 1e30f, vz = 1e30f;  // padding: never a hit
             if (k < nch && j <= e) {
-              double4 xj = d.pos[j];
+              const double4 xj = ld_pos<DIM>(d.pos + j);
               vx = (float)(xj.x + sx - ox);
               vy = (float)(xj.y + sy - oy);
               vz = (float)(xj.z + sz - oz);
@@ -633,7 +633,7 @@ __global__ void k_density(Dev d) {
   const T h[3] = {(T)p.halfL[0], (T)p.halfL[1], (T)p.halfL[2]};
   const T rcutsq = (T)p.rcutsq;
   const T rcut_inv = (T)p.rcut_inv, cw = (T)p.cw;
-  const V xi = P[i];
+  const V xi = ld_pos<DIM>(P + i);
   const int n = min(d.nbr_cnt[i], d.cap);
   // the particle's list row, read four indices at a time one batch ahead
   const int4* __restrict__ row = reinterpret_cast<const int4*>(d.nbr + (size_t)i * d.cap);
@@ -647,7 +647,7 @@ __global__ void k_density(Dev d) {
     for (int q = 0; q < 4; ++q) {
       if (q >= m) break;
       const int j = q == 0 ? cur.x : q == 1 ? cur.y : q == 2 ? cur.z : cur.w;
-      const T w = density_term<T, DIM>(xi, P[j], L, h, p.wall, rcutsq, rcut_inv, cw);
+      const T w = density_term<T, DIM>(xi, ld_pos<DIM>(P + j), L, h, p.wall, rcutsq, rcut_inv, cw);
       if constexpr (Compensated<T>::on)
         kahan_add(dens, comp, w);
       else
