@@ -584,7 +584,7 @@ def main():
     if args.pairs_traffic is None and args.lattice == 128 and args.precision in (None, "fp64"):
         # dram__bytes_read.sum + dram__bytes_write.sum of one k_pairs launch at 96^3
         # (940,032 particles), scaled to the 2,195,456 particles of the benchmark
-        args.pairs_traffic = (722.530304e6 + 66.258944e6) * 2195456 / 940032
+        args.pairs_traffic = (724.24448e6 + 64.03584e6) * 2195456 / 940032
     if args.precision is None:
         args.precision = "mixed" if args.workload == "sweep" else "fp64"
     if args.lattice != 128:
