@@ -85,6 +85,39 @@ def test_fp64_engine_matches_oracle(name, workdir):
     assert e.kernel_launches() > 0
 
 
+LONG = {
+    # config 1 at its own size: 2D Kolmogorov flow, 64^2 = 4,096 particles
+    "kolmogorov64": (dict(N=(64, 64), L=(1.0, 1.0), dim=2, overlap=4.0, ext_force_type=2,
+                          ext_force=(1.0, 0.0), dt=5e-5), 200),
+    "couette2d": (mg.CASES["couette2d"], 100),
+    "colloids2d": (mg.CASES["colloids2d"], 100),
+    "colloids3d": (mg.CASES["colloids3d"], 30),
+}
+
+
+@pytest.mark.parametrize("name", list(LONG))
+def test_fp64_engine_matches_oracle_after_n_steps(name, workdir):
+    """FP64 engine against the FP64 oracle after N steps (the oracle is built without FMA
+    contraction, the engine with it).  Tolerance 1e-9 of each field group's scale."""
+    spec, nsteps = LONG[name]
+    inp = os.path.join(workdir, "input")
+    sph_input.write_input(inp, **spec)
+    e = sph_b200.System(inp)
+    o = oracle.Oracle(inp)
+    o.run(0)
+    e.step(0)
+    o.run(nsteps)
+    e.step(nsteps)
+    e.synchronize()
+    errs = compare_state(e, o, 1e-9, "step%d" % nsteps)
+    cells = e.export_cells()
+    for k in INTS:
+        assert np.array_equal(cells[k], o.ifield(k)), k
+    assert e.info()["step"] == nsteps, errs
+    e.close()
+    o.close()
+
+
 @pytest.mark.parametrize("name", list(mg.CASES))
 def test_mixed_engine_matches_oracle(name, workdir):
     e, o = open_case(name, workdir, precision="mixed")
