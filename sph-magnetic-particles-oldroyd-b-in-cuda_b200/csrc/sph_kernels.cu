@@ -432,6 +432,31 @@ __global__ void __launch_bounds__(kListWarps * 32) k_build_lists(Dev d) {
     const f32x2 cut22 = f2_pack(cut2, cut2);
     int* rowp = d.nbr + (size_t)(active ? i : 0) * cap;
     int cnt = 0;
+    // the neighbour cells' candidate ranges: with a warp per cell, lane q loads those of
+    // neighbour cell q up front (all 3^d loads in flight at once) and the loop takes them
+    // by shuffle; a half-warp group loads them as it goes
+    constexpr int kNZ = DIM == 3 ? 3 : 1;
+    int rs = 0, re = -1;
+    if (TPC == 32 && live && lane < 9 * kNZ) {
+      const int ddx = lane / (3 * kNZ) - 1, ddy = (lane / kNZ) % 3 - 1;
+      const int ddz = DIM == 3 ? lane % 3 - 1 : 0;
+      int nx = cx + ddx, ny = cy + ddy, nz = cz + ddz;
+      if (nx < 0) nx += N0;
+      if (nx >= N0) nx -= N0;
+      if (DIM == 3) {
+        if (nz < 0) nz += N2;
+        if (nz >= N2) nz -= N2;
+      }
+      if (!p.wall) {
+        if (ny < 0) ny += N1;
+        if (ny >= N1) ny -= N1;
+      }
+      if (ny >= 0 && ny < N1) {
+        const int nc = p.cell0 + (DIM == 3 ? (nz * N1 + ny) * N0 + nx : ny * N0 + nx);
+        rs = d.cell_start[nc] + p.slot0;
+        re = d.cell_end[nc] + p.slot0;
+      }
+    }
     for (int ddx = -1; ddx <= 1; ++ddx)
       for (int ddy = -1; ddy <= 1; ++ddy)
         for (int ddz = (DIM == 3 ? -1 : 0); ddz <= (DIM == 3 ? 1 : 0); ++ddz) {
@@ -449,7 +474,11 @@ __global__ void __launch_bounds__(kListWarps * 32) k_build_lists(Dev d) {
           }
           // an empty range where the neighbour row does not exist (walls) or the group idles
           int s = 0, e = -1;
-          if (live && ny >= 0 && ny < N1) {
+          if (TPC == 32) {
+            const int q = ((ddx + 1) * 3 + (ddy + 1)) * kNZ + (DIM == 3 ? ddz + 1 : 0);
+            s = __shfl_sync(SPH_FULL, rs, q);
+            e = __shfl_sync(SPH_FULL, re, q);
+          } else if (live && ny >= 0 && ny < N1) {
             const int nc = p.cell0 + (DIM == 3 ? (nz * N1 + ny) * N0 + nx : ny * N0 + nx);
             s = d.cell_start[nc] + p.slot0;
             e = d.cell_end[nc] + p.slot0;
