@@ -70,6 +70,22 @@ B_ALG_STEP = {"fp64": (10 * 3 + 5 * 6 + 4) * 8 + 28, "mixed": 380}
 # f (3) and dc/dt (6).
 B_ALG_PAIRS = {"fp64": (6 + 6 + 1 + 1 + 6 + 1 + 3 + 6) * 8 + 4,
                "mixed": (6 + 6 + 1) * 4 + (1 + 6 + 1 + 3 + 6) * 8 + 4}
+# FP64 floating-point operations per particle of one launch of the FP64 pair kernel, counted
+# by ncu on the 96^3 case of this workload (same lattice, same neighbours per particle):
+# DADD + DMUL + 2 DFMA thread instructions / particles (profiles/k_pairs_couette96_fp64.md).
+FP64_PAIR_FLOP = 11842.3
+# FP64 peak of the B200: 148 SMs x 64 FP64 FMA lanes (ncu's dfma peak_sustained, 9,472 per
+# cycle) x 2 FLOP x the SM clock.
+FP64_LANES = 9472
+
+
+def clock_mhz():
+    """Maximum SM clock of this pool's B200s (MEASURED_PEAKS.json), else the nominal 1965 MHz."""
+    path = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    if os.path.exists(path):
+        with open(path) as f:
+            return float(json.load(f).get("sm_max_mhz", 1965.0))
+    return 1965.0
 
 
 def peaks():
@@ -302,6 +318,13 @@ def run_ours(args, world, rank, local, dist):
                              "fraction is reported as the metric asks"},
         "hbm_frac_step": step_gbs / hbm,
         "phase_ms": phases,
+        "roofline_fp64": None if args.precision != "fp64" else {
+            "kernel": "k_pairs", "bound": "fp64",
+            "achieved": FP64_PAIR_FLOP * n / (pair_ms * 1e-3) / 1e12,
+            "peak": FP64_LANES * 2 * clock_mhz() * 1e6 / 1e12, "unit": "TFLOP/s",
+            "frac": FP64_PAIR_FLOP * n / (pair_ms * 1e-3) / (FP64_LANES * 2 * clock_mhz() * 1e6),
+            "note": "executed FP64 FLOP per particle counted by ncu (DADD + DMUL + 2 DFMA) over "
+                    "the event-timed pair pass; peak = 9,472 FP64 FMA lanes x 2 x SM clock"},
         "e2e": {"value": n * e2e_steps / e2e_dt, "unit": UNIT, "h2d_bytes_per_step": 24,
                 "d2h_bytes_per_step": 2 * 3 * 8 + 8, "steps": e2e_steps},
         "gpu_launches": launches,
