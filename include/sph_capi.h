@@ -266,7 +266,9 @@ sph_status sph_reset_observables(sph_ctx* ctx);
    depend on it, bit for bit):
      list_threads_per_cell  32: a warp per cell in the list build; 16: a half-warp per
                             cell (2D cells at overlap 4 hold about 16 particles)
-     density_block          threads per block of the density pass: 64, 128 or 256
+     density_block          0: the density pass over neighbour-cell tiles (a warp per cell,
+                            the cells' positions staged in shared memory); 64, 128 or 256:
+                            threads per block of the per-particle density pass
    sph_set_tuning applies a geometry (captured step graphs are rebuilt).  sph_autotune
    times the candidates on the context's current state -- the timed passes recompute the
    same lists and densities, so the simulation is unchanged -- and keeps the fastest.

@@ -1301,7 +1301,8 @@ namespace {
 
 bool tuning_ok(const sph_tuning& t) {
   return (t.list_threads_per_cell == 32 || t.list_threads_per_cell == 16) &&
-         (t.density_block == 64 || t.density_block == 128 || t.density_block == 256);
+         (t.density_block == 0 || t.density_block == 64 || t.density_block == 128 ||
+          t.density_block == 256);
 }
 
 // Cache key: GPU name, dimension, overlap of the first box, total particles rounded to a
@@ -1439,7 +1440,7 @@ sph_status sph_autotune(sph_ctx* c, const char* cache_path, sph_tuning* chosen) 
       best.list_threads_per_cell = tpc;
     }
   }
-  for (int nt : {64, 128, 256}) {
+  for (int nt : {0, 64, 128, 256}) {  // 0: neighbour-cell tiles
     Launch L = launcher(c);
     L.density_block = nt;
     const double ms = time_phase(c, reps, [&] { return launch_density_dim(L, c->dim); }, &bad);

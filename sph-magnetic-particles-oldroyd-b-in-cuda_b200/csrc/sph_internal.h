@@ -193,7 +193,7 @@ struct Launch {
   void* stream;
   long long* launches;
   int list_tpc = 32;        // threads per cell of the list build (32 or 16)
-  int density_block = 128;  // threads per block of the density pass (64, 128 or 256)
+  int density_block = 128;  // density pass: 0 = neighbour-cell tiles, else threads per block
   // (launch geometry only: results do not depend on it)
 };
 

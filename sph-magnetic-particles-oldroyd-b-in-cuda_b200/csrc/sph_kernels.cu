@@ -686,6 +686,142 @@ __global__ void k_density(Dev d) {
   density_epilogue<T>(d, i, p, (double)dens - (double)comp);
 }
 
+// Density over neighbour-cell tiles: one warp per cell, as the list build.  The positions
+// of the neighbour cells' candidate ranges (the list build's ranges, stale ones included)
+// are staged in shared memory by coalesced copies, in phases of 9 cells (the dx = -1, 0, +1
+// planes in 3D; all 9 cells at once in 2D), and every lane walks its own list in order,
+// reading each neighbour from the tile.  The sums are those of k_density term for term:
+// the same list order, the same arithmetic; only where the position is read from differs.
+// An entry outside the staged ranges (a tile overflow, or a particle listed from other
+// cells because it sits exactly on the upper box edge) reads its position from global
+// memory in place, so the order is never changed.
+constexpr int kDensWarps = 4;
+constexpr int kDensTile = 320;  // staged positions per warp and phase
+
+template <typename T, int DIM>
+__global__ void __launch_bounds__(kDensWarps * 32) k_density_cells(Dev d) {
+  using V = typename V4<T>::type;
+  constexpr int kNZ = DIM == 3 ? 3 : 1;
+  constexpr int kNR = 9 * kNZ;               // neighbour cells
+  constexpr int kPh = DIM == 3 ? 3 : 1;      // phases
+  constexpr int kPerPh = kNR / kPh;          // cells per phase (9)
+  __shared__ T tx[kDensWarps][kDensTile], ty[kDensWarps][kDensTile], tz[kDensWarps][kDensTile];
+  __shared__ int rtab[kDensWarps][kPerPh][3];  // per phase: first slot, last slot, tile offset
+  const int w = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const int cell = blockIdx.x * kDensWarps + w;
+  if (cell >= d.Ctot) return;  // whole warps only
+  const V* __restrict__ P = sizeof(T) == 8 ? reinterpret_cast<const V*>(d.pos)
+                                           : reinterpret_cast<const V*>(d.pos_f);
+  const int b = d.cell_box[cell];
+  const BoxParams& p = d.box[b];
+  const int N0 = p.Ncells[0], N1 = p.Ncells[1], N2 = p.Ncells[2];
+  const int lc = cell - p.cell0;
+  const int cx = lc % N0, cy = (lc / N0) % N1, cz = DIM == 3 ? lc / (N0 * N1) : 0;
+  // candidate range of neighbour cell `lane` (the list build's, kernel_densities.cu:52-163)
+  int rs = 0, re = -1;
+  if (lane < kNR) {
+    const int ddx = lane / (3 * kNZ) - 1, ddy = (lane / kNZ) % 3 - 1;
+    const int ddz = DIM == 3 ? lane % 3 - 1 : 0;
+    int nx = cx + ddx, ny = cy + ddy, nz = cz + ddz;
+    if (nx < 0) nx += N0;
+    if (nx >= N0) nx -= N0;
+    if (DIM == 3) {
+      if (nz < 0) nz += N2;
+      if (nz >= N2) nz -= N2;
+    }
+    if (!p.wall) {
+      if (ny < 0) ny += N1;
+      if (ny >= N1) ny -= N1;
+    }
+    if (ny >= 0 && ny < N1) {
+      const int nc = p.cell0 + (DIM == 3 ? (nz * N1 + ny) * N0 + nx : ny * N0 + nx);
+      rs = d.cell_start[nc] + p.slot0;
+      re = d.cell_end[nc] + p.slot0;
+    }
+  }
+  const int rcount = re >= rs ? re - rs + 1 : 0;
+  const T L[3] = {(T)p.L[0], (T)p.L[1], (T)p.L[2]};
+  const T h[3] = {(T)p.halfL[0], (T)p.halfL[1], (T)p.halfL[2]};
+  const T rcutsq = (T)p.rcutsq;
+  const T rcut_inv = (T)p.rcut_inv, cw = (T)p.cw;
+  const int beg = d.cell_begin[cell], end = d.cell_begin[cell + 1];
+  for (int t0 = 0; t0 < end - beg; t0 += 32) {
+    const int i = beg + t0 + lane;
+    const bool active = i < end;
+    const V xi = active ? ld_pos<DIM>(P + i) : V{};
+    const int n = active ? min(d.nbr_cnt[i], d.cap) : 0;
+    const int* __restrict__ row = d.nbr + (size_t)(active ? i : 0) * d.cap;
+    T dens = T(0), comp = T(0);  // comp: Kahan compensation of a float sum
+    auto add = [&](const V& xj) {
+      const T wv = density_term<T, DIM>(xi, xj, L, h, p.wall, rcutsq, rcut_inv, cw);
+      if constexpr (Compensated<T>::on)
+        kahan_add(dens, comp, wv);
+      else
+        dens = dens + wv;
+    };
+    int k = 0;
+    for (int ph = 0; ph < kPh; ++ph) {
+      // tile offsets of this phase's ranges: exclusive prefix over lanes ph*9 .. ph*9+8
+      const bool mine = lane >= ph * kPerPh && lane < (ph + 1) * kPerPh;
+      int off = mine ? rcount : 0;
+#pragma unroll
+      for (int o = 1; o < 32; o <<= 1) {
+        const int v = __shfl_up_sync(SPH_FULL, off, o);
+        if (lane >= o) off += v;
+      }
+      off -= mine ? rcount : 0;
+      if (mine) {
+        rtab[w][lane - ph * kPerPh][0] = rs;
+        rtab[w][lane - ph * kPerPh][1] = re;
+        rtab[w][lane - ph * kPerPh][2] = off;
+      }
+      // stage the phase's ranges (coalesced), up to the tile capacity
+#pragma unroll 1
+      for (int q = 0; q < kPerPh; ++q) {
+        const int qs = __shfl_sync(SPH_FULL, rs, ph * kPerPh + q);
+        const int qn = __shfl_sync(SPH_FULL, rcount, ph * kPerPh + q);
+        const int qo = __shfl_sync(SPH_FULL, off, ph * kPerPh + q);
+        for (int u = lane; u < qn && qo + u < kDensTile; u += 32) {
+          const V x = ld_pos<DIM>(P + qs + u);
+          tx[w][qo + u] = x.x;
+          ty[w][qo + u] = x.y;
+          if (DIM == 3) tz[w][qo + u] = x.z;
+        }
+      }
+      __syncwarp();
+      // this lane's list entries that fall in the phase's ranges, in list order
+      int qc = 0;
+      int qs = rtab[w][0][0], qe = rtab[w][0][1], qo = rtab[w][0][2];
+      while (k < n) {
+        const int j = __ldg(&row[k]);
+        while (qc < kPerPh && (j < qs || j > qe)) {
+          if (++qc < kPerPh) {
+            qs = rtab[w][qc][0];
+            qe = rtab[w][qc][1];
+            qo = rtab[w][qc][2];
+          }
+        }
+        if (qc == kPerPh) break;  // a later phase's entry
+        const int t = qo + (j - qs);
+        V xj;
+        if (t < kDensTile) {
+          xj.x = tx[w][t];
+          xj.y = ty[w][t];
+          xj.z = DIM == 3 ? tz[w][t] : T(0);
+        } else {
+          xj = ld_pos<DIM>(P + j);
+        }
+        add(xj);
+        ++k;
+      }
+      __syncwarp();  // the tile and the range table are refilled by the next phase
+    }
+    // entries from no staged range: global reads, still in list order
+    for (; k < n; ++k) add(ld_pos<DIM>(P + __ldg(&row[k])));
+    if (active) density_epilogue<T>(d, i, p, (double)dens - (double)comp);
+  }
+}
+
 // kernel_pressures.cu:13-23 (standalone, also refreshes the neighbour record)
 template <typename T>
 __global__ void k_pressure(Dev d) {
@@ -1375,6 +1511,19 @@ int launch_colloid_cells_n(const Launch& L, int nboxes, int max_coll) {
 
 int launch_density_dim(const Launch& L, int dim) {
   if (L.d.Ntot == 0) return 0;
+  if (L.density_block == 0) {
+    // neighbour-cell tiles, one warp per cell
+    const int nb = blocks(L.d.Ctot, kDensWarps);
+    constexpr int nt = kDensWarps * 32;
+    if (L.prec == SPH_PREC_FP64) {
+      if (dim == 3) k_density_cells<double, 3><<<nb, nt, 0, S(L)>>>(L.d);
+      else k_density_cells<double, 2><<<nb, nt, 0, S(L)>>>(L.d);
+    } else {
+      if (dim == 3) k_density_cells<float, 3><<<nb, nt, 0, S(L)>>>(L.d);
+      else k_density_cells<float, 2><<<nb, nt, 0, S(L)>>>(L.d);
+    }
+    return check(L);
+  }
   const int nt = L.density_block;
   const int nb = blocks(L.d.Ntot, nt);
   if (L.prec == SPH_PREC_FP64) {

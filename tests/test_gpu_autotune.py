@@ -26,7 +26,7 @@ def _input(workdir, name, **over):
 def test_geometries_give_identical_bits(workdir, case):
     p = _input(workdir, case)
     runs = []
-    for tpc, blk in [(32, 128), (16, 64), (16, 256), (32, 256)]:
+    for tpc, blk in [(32, 128), (16, 64), (16, 256), (32, 256), (32, 0), (16, 0)]:
         s = sph_b200.System(p)
         s.set_tuning(tpc, blk)
         assert s.tuning() == {"list_threads_per_cell": tpc, "density_block": blk}
@@ -37,6 +37,28 @@ def test_geometries_give_identical_bits(workdir, case):
     for r in runs[1:]:
         for f in FIELDS:
             assert np.array_equal(r[f], runs[0][f]), f
+
+
+@pytest.mark.parametrize("precision", ["fp64", "mixed"])
+def test_3d_density_tiles_identical(workdir, precision):
+    """The density pass over neighbour-cell tiles against the per-particle pass, in 3D with
+    colloids (stale and empty cells inside them) and at overlap 4, where 9 cells of 64
+    particles overflow the tile and the overflow is read from global memory."""
+    p3 = _input(workdir, "colloids3d")
+    p4 = os.path.join(workdir, "input_ov4")
+    sph_input.write_input(p4, N=(24, 24, 24), L=(1.0, 1.0, 1.0), dim=3, overlap=4.0, wall=1,
+                          Vwall_bottom=-0.3, Vwall_top=0.3, dt=2e-5)
+    for p in (p3, p4):
+        out = []
+        for blk in (128, 0):
+            s = sph_b200.System(p, precision=precision)
+            s.set_tuning(32, blk)
+            s.step(3)
+            s.synchronize()
+            out.append([s.field(f) for f in ("x", "vx", "fz", "dens", "press")])
+            s.close()
+        for a, b in zip(*out):
+            assert np.array_equal(a, b)
 
 
 def test_3d_half_warp_lists_identical(workdir):
