@@ -524,25 +524,24 @@ __device__ __forceinline__ void pair_term(const BoxParams& p, const PairParams<T
       kahan_add(acc.f[0], acc.cf[0], t0 + (aux1 * v[0] + aux2 * e[0]));
       kahan_add(acc.f[1], acc.cf[1], t1 + (aux1 * v[1] + aux2 * e[1]));
       if (DIM == 3) kahan_add(acc.f[2], acc.cf[2], t2 + (aux1 * v[2] + aux2 * e[2]));
-    } else if (DIM == 2) {
-      const T ev = e[0] * v[0] + e[1] * v[1];
-      acc.f[0] += axx * e[0] + axy * e[1];
-      acc.f[1] += axy * e[0] + ayy * e[1];
-      const T aux2 = pp.b * aux * ev;
-      acc.f[0] += aux1 * v[0] + aux2 * e[0];
-      acc.f[1] += aux1 * v[1] + aux2 * e[1];
     } else {
-      const T axz = -gw * (Pi[3] + Pj[3]);
-      const T ayz = -gw * (Pi[4] + Pj[4]);
-      const T azz = -gw * (Pi[5] + Pj[5]);
-      const T ev = e[0] * v[0] + e[1] * v[1] + e[2] * v[2];
-      acc.f[0] += axx * e[0] + axy * e[1] + axz * e[2];
-      acc.f[1] += axy * e[0] + ayy * e[1] + ayz * e[2];
-      acc.f[2] += axz * e[0] + ayz * e[1] + azz * e[2];
+      // -gw (Pi + Pj).e and the viscous terms folded into the sums by fused multiply-adds
+      const T ngw = -gw;
+      T ev = e[0] * v[0] + e[1] * v[1];
+      T t0 = (Pi[0] + Pj[0]) * e[0] + (Pi[1] + Pj[1]) * e[1];
+      T t1 = (Pi[1] + Pj[1]) * e[0] + (Pi[2] + Pj[2]) * e[1];
+      T t2 = T(0);
+      if (DIM == 3) {
+        const T sxz = Pi[3] + Pj[3], syz = Pi[4] + Pj[4];
+        ev += e[2] * v[2];
+        t0 += sxz * e[2];
+        t1 += syz * e[2];
+        t2 = sxz * e[0] + syz * e[1] + (Pi[5] + Pj[5]) * e[2];
+      }
       const T aux2 = pp.b * aux * ev;
-      acc.f[0] += aux1 * v[0] + aux2 * e[0];
-      acc.f[1] += aux1 * v[1] + aux2 * e[1];
-      acc.f[2] += aux1 * v[2] + aux2 * e[2];
+      acc.f[0] = fma(aux2, e[0], fma(aux1, v[0], fma(ngw, t0, acc.f[0])));
+      acc.f[1] = fma(aux2, e[1], fma(aux1, v[1], fma(ngw, t1, acc.f[1])));
+      if (DIM == 3) acc.f[2] = fma(aux2, e[2], fma(aux1, v[2], fma(ngw, t2, acc.f[2])));
     }
   }
 }
