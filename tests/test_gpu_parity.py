@@ -245,6 +245,29 @@ def test_forces_store_the_same_gradient_as_the_gradient_pass(name, workdir):
     e.close()
 
 
+@pytest.mark.parametrize("precision", ["fp64", "mixed"])
+def test_neighbour_capacity_grows(precision, workdir):
+    """Neighbour lists that start far too short (16 slots where about 100 are needed)
+    overflow, are detected on the device, grow and are rebuilt: the run is bit-identical to
+    one with the derived capacity, through the step graph and through the step methods."""
+    mg.case_dir("colloids3d", workdir)
+    inp = os.path.join(workdir, "input")
+    ref = sph_b200.System(inp, precision=precision)
+    small = sph_b200.System(inp, precision=precision, nbr_capacity=16)
+    for s in (ref, small):
+        s.step(3)
+        s.V_Verlet_step1()
+        s.neighbours_search()
+        s.calculate_forces(np.array([0.2, 0.1, 0.0]))
+        s.V_Verlet_step2()
+        s.synchronize()
+    for f in ["x", "y", "z", "vx", "fx", "dens", "cxy"]:
+        assert np.array_equal(small.field(f), ref.field(f)), f
+    assert np.array_equal(small.wall_forces(), ref.wall_forces())
+    small.close()
+    ref.close()
+
+
 def test_device_errors_are_reported_not_trapped(workdir):
     """A non-finite position and a particle outside the wall band come back as statuses;
     the context keeps working once the state is repaired."""
@@ -383,3 +406,11 @@ def test_full_size_couette_128(workdir):
         assert err <= MIXED_TOL[gname], (gname, err)
     wa, wb = a.wall_forces(), b.wall_forces()
     assert np.abs(wa - wb).max() <= 2e-5 * np.abs(wa).max()
+    # the chunked wall reduction (49,152 particles per wall, 96 chunks) against a host sum
+    # of the wall particles' forces (system_calculate_force_walls.cu:15-38)
+    t = a.type()
+    f = np.stack([a.field("fx"), a.field("fy"), a.field("fz")], axis=1)
+    for w in (1, 2):
+        ref = f[t == w].sum(axis=0)
+        scale = np.abs(f[t == w]).sum(axis=0).max()
+        assert np.abs(wa[0, w - 1] - ref).max() <= 1e-12 * scale, (w, wa[0, w - 1], ref)
