@@ -17,9 +17,25 @@ template <typename T> struct V4;
 template <> struct V4<double> { using type = double4; };
 template <> struct V4<float> { using type = float4; };
 
-template <typename T> struct RecOf;
-template <> struct RecOf<double> { using type = RecD; };
-template <> struct RecOf<float> { using type = RecF; };
+template <typename T, int DIM> struct RecFor;
+template <> struct RecFor<double, 3> { using type = RecD; };
+template <> struct RecFor<float, 3> { using type = RecF; };
+template <> struct RecFor<double, 2> { using type = RecD2; };
+template <> struct RecFor<float, 2> { using type = RecF2; };
+
+// Fields a 2D record does not carry read as zero.
+template <int DIM, typename R>
+__device__ __forceinline__ auto rec_z(const R& r) -> decltype(r.x) {
+  if constexpr (DIM == 3) return r.z; else return decltype(r.x)(0);
+}
+template <int DIM, typename R>
+__device__ __forceinline__ auto rec_vz(const R& r) -> decltype(r.x) {
+  if constexpr (DIM == 3) return r.vz; else return decltype(r.x)(0);
+}
+template <int DIM, typename R>
+__device__ __forceinline__ auto rec_P(const R& r, int q) -> decltype(r.x) {
+  if constexpr (DIM == 3) return r.P[q]; else return q < 3 ? r.P[q] : decltype(r.x)(0);
+}
 
 // ---------------------------------------------------------------------------------
 // SPH kernel and its radial derivative (kernel_W.cu:13-59, kernel_gradW.cu:13-53).
@@ -124,38 +140,42 @@ __device__ __forceinline__ void raise_status(const Dev& d, unsigned bit, int inf
 }
 
 
-template <typename T>
+template <typename T, int DIM>
 __device__ __forceinline__ void write_record(const Dev& d, int i, const BoxParams& p, int ti,
                                              double dens, double press) {
-  using Rec = typename RecOf<T>::type;
+  using Rec = typename RecFor<T, DIM>::type;
+  constexpr int kP = DIM == 3 ? 6 : 3;  // stress components carried
   Rec* rec = reinterpret_cast<Rec*>(d.rec);
   const int Np = d.Npad;
   const double4 x = d.pos[i];
   const double4 v = d.vel[i];
   Rec r;
-  r.x = x.x; r.y = x.y; r.z = x.z;
-  r.vx = v.x; r.vy = v.y; r.vz = v.z;
+  r.x = x.x; r.y = x.y;
+  r.vx = v.x; r.vy = v.y;
+  if constexpr (DIM == 3) {
+    r.z = x.z;
+    r.vz = v.z;
+    r.tinfo = ti;
+  }
   const double nkT = p.nkT;
   double c[6];
 #pragma unroll
-  for (int q = 0; q < 6; ++q) c[q] = d.conf[q * Np + i];
+  for (int q = 0; q < kP; ++q) c[q] = d.conf[q * Np + i];
   const double dinv = 1.0 / dens;
   if (type_of(ti) == 0) {
-    // Pi / d^2 with Pi = p I - nkT c (kernel_forces.cu:62-88)
+    // Pi / d^2 with Pi = p I - nkT c (kernel_forces.cu:62-88); diagonal: xx, yy, zz
     const double dsq = dinv * dinv;
-    r.P[0] = (T)((press - nkT * c[0]) * dsq);
-    r.P[1] = (T)((-nkT * c[1]) * dsq);
-    r.P[2] = (T)((press - nkT * c[2]) * dsq);
-    r.P[3] = (T)((-nkT * c[3]) * dsq);
-    r.P[4] = (T)((-nkT * c[4]) * dsq);
-    r.P[5] = (T)((press - nkT * c[5]) * dsq);
+#pragma unroll
+    for (int q = 0; q < kP; ++q) {
+      const bool diag = q == 0 || q == 2 || q == 5;
+      r.P[q] = diag ? (T)((press - nkT * c[q]) * dsq) : (T)((-nkT * c[q]) * dsq);
+    }
   } else {
     // walls / colloid particles: -nkT c, completed with the fluid partner's p and d
 #pragma unroll
-    for (int q = 0; q < 6; ++q) r.P[q] = (T)(-nkT * c[q]);
+    for (int q = 0; q < kP; ++q) r.P[q] = (T)(-nkT * c[q]);
   }
   r.invd = (T)dinv;
-  r.tinfo = ti;
   rec[i] = r;
 }
 
@@ -407,19 +427,21 @@ struct PairAcc {
   }
 };
 
+// ti: the particle's type word (from the type array)
 template <typename T, int DIM, int MODE, typename Rec>
-__device__ __forceinline__ void load_own(const Dev& d, int i, const Rec& ri, PairOwn<T, DIM>& o) {
+__device__ __forceinline__ void load_own(const Dev& d, int i, int ti, const Rec& ri,
+                                         PairOwn<T, DIM>& o) {
   o.x = (T)ri.x;
   o.y = (T)ri.y;
-  o.z = (T)ri.z;
+  o.z = (T)rec_z<DIM>(ri);
   o.v[0] = (T)ri.vx;
   o.v[1] = (T)ri.vy;
-  o.v[2] = DIM == 3 ? (T)ri.vz : T(0);
+  o.v[2] = (T)rec_vz<DIM>(ri);
   o.invd = ri.invd;
   o.press = (T)d.press[i];
 #pragma unroll
-  for (int q = 0; q < 6; ++q) o.P[q] = ri.P[q];
-  o.t = type_of(ri.tinfo);
+  for (int q = 0; q < 6; ++q) o.P[q] = rec_P<DIM>(ri, q);
+  o.t = type_of(ti);
   o.fluid = o.t == 0;
   // gradient: every particle in kPairGradvAll; in the fused pass fluid particles (whose
   // dc/dt needs it), or every particle when the caller stores the whole field
@@ -427,21 +449,21 @@ __device__ __forceinline__ void load_own(const Dev& d, int i, const Rec& ri, Pai
   o.do_force = MODE != kPairGradvAll;
 }
 
+// tj: the neighbour's particle type
 template <typename T, int DIM, typename Rec>
 __device__ __forceinline__ void pair_term(const BoxParams& p, const PairParams<T, DIM>& pp,
                                           const CollView& cv, const PairOwn<T, DIM>& o,
-                                          const Rec& rj, PairAcc<T, DIM>& acc) {
-  const int tj = type_of(rj.tinfo);
+                                          const Rec& rj, int tj, PairAcc<T, DIM>& acc) {
   const bool fluid_j = tj == 0;
   // skip rules: gradient kernel_vel_gradients.cu:126-127, forces kernel_forces.cu:157-158
   const bool pair_grad = o.do_grad && !(o.t == tj && !o.fluid);
   const bool pair_force = o.do_force && (o.fluid || fluid_j);
   if (!pair_grad && !pair_force) return;
-  T r[3] = {o.x - (T)rj.x, o.y - (T)rj.y, DIM == 3 ? o.z - (T)rj.z : T(0)};
+  T r[3] = {o.x - (T)rj.x, o.y - (T)rj.y, DIM == 3 ? o.z - (T)rec_z<DIM>(rj) : T(0)};
   min_image<T, DIM>(r[0], r[1], r[2], pp.L, pp.h, p.wall);
   const T r2 = DIM == 3 ? r[0] * r[0] + r[1] * r[1] + r[2] * r[2] : r[0] * r[0] + r[1] * r[1];
   if (!(r2 < pp.rcutsq)) return;
-  const T vj[3] = {(T)rj.vx, (T)rj.vy, DIM == 3 ? (T)rj.vz : T(0)};
+  const T vj[3] = {(T)rj.vx, (T)rj.vy, (T)rec_vz<DIM>(rj)};
   T v[3];
   if (o.t == tj) {
     v[0] = o.v[0] - vj[0];
@@ -450,7 +472,7 @@ __device__ __forceinline__ void pair_term(const BoxParams& p, const PairParams<T
   } else if (o.fluid) {
     ghost_fluid_i<T, DIM>(p, cv, tj, p.coll0, o.x, o.y, o.z, (T)rj.y, o.v, r, pp.L, pp.h, v);
   } else {
-    ghost_solid_i<T, DIM>(p, cv, o.t, p.coll0, o.y, (T)rj.x, (T)rj.y, (T)rj.z, vj, r, pp.L,
+    ghost_solid_i<T, DIM>(p, cv, o.t, p.coll0, o.y, (T)rj.x, (T)rj.y, (T)rec_z<DIM>(rj), vj, r, pp.L,
                           pp.h, v);
   }
   const T rinv = rsqrt(r2);  // r and 1/r from one reciprocal square root
@@ -477,7 +499,7 @@ __device__ __forceinline__ void pair_term(const BoxParams& p, const PairParams<T
 #pragma unroll
       for (int q = 0; q < 6; ++q) {
         Pi[q] = o.P[q];
-        Pj[q] = rj.P[q];
+        Pj[q] = rec_P<DIM>(rj, q);
       }
       di = o.invd;
       dj = rj.invd;
@@ -488,7 +510,7 @@ __device__ __forceinline__ void pair_term(const BoxParams& p, const PairParams<T
       for (int q = 0; q < 6; ++q) {
         Pi[q] = o.P[q];
         const T diag = (q == 0 || q == 2 || q == 5) ? o.press : T(0);
-        Pj[q] = (diag + rj.P[q]) * dsq;
+        Pj[q] = (diag + rec_P<DIM>(rj, q)) * dsq;
       }
       di = o.invd;
       dj = o.invd;
@@ -496,8 +518,8 @@ __device__ __forceinline__ void pair_term(const BoxParams& p, const PairParams<T
       // i takes j's density, pressure and c (kernel_forces.cu:320-336)
 #pragma unroll
       for (int q = 0; q < 6; ++q) {
-        Pj[q] = rj.P[q];
-        Pi[q] = rj.P[q];
+        Pj[q] = rec_P<DIM>(rj, q);
+        Pi[q] = rec_P<DIM>(rj, q);
       }
       di = rj.invd;
       dj = rj.invd;

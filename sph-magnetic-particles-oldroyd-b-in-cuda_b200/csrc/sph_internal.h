@@ -112,6 +112,22 @@ struct alignas(16) RecF {
 };
 static_assert(sizeof(RecF) == 64, "RecF layout");
 
+// 2D records: only the fields a 2D pair term reads (P = xx, xy, yy); the type word is read
+// from the slot-ordered type array.  Half the bytes of the 3D records to stage per pair.
+struct alignas(16) RecD2 {
+  double x, y, vx, vy;
+  double P[3];
+  double invd;
+};
+static_assert(sizeof(RecD2) == 64, "RecD2 layout");
+
+struct alignas(16) RecF2 {
+  float x, y, vx, vy;
+  float P[3];
+  float invd;
+};
+static_assert(sizeof(RecF2) == 32, "RecF2 layout");
+
 // Device pointers, passed to kernels by value.
 struct Dev {
   int Ntot, Npad, nboxes, Ctot, ncoll, nwallseg, cap;

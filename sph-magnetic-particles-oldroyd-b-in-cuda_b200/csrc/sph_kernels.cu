@@ -301,13 +301,13 @@ __device__ __forceinline__ T density_term(const typename V4<T>::type& xi,
 }
 
 // Density, pressure (kernel_pressures.cu:13-23) and the neighbour record of slot i.
-template <typename T>
+template <typename T, int DIM>
 __device__ __forceinline__ void density_epilogue(const Dev& d, int i, const BoxParams& p,
                                                  double dens) {
   d.dens[i] = dens;
   const double press = p.csq * (d.pos[i].w * dens - p.rho0);
   d.press[i] = press;
-  write_record<T>(d, i, p, d.tinfo[i], dens, press);
+  write_record<T, DIM>(d, i, p, d.tinfo[i], dens, press);
 }
 
 // One warp per cell: the cell's particles (<= 32 per round) test the candidates of the
@@ -683,7 +683,7 @@ __global__ void k_density(Dev d) {
         dens = dens + w;
     }
   }
-  density_epilogue<T>(d, i, p, (double)dens - (double)comp);
+  density_epilogue<T, DIM>(d, i, p, (double)dens - (double)comp);
 }
 
 // Density over neighbour-cell tiles: one warp per cell, as the list build.  The positions
@@ -818,7 +818,7 @@ __global__ void __launch_bounds__(kDensWarps * 32) k_density_cells(Dev d) {
     }
     // entries from no staged range: global reads, still in list order
     for (; k < n; ++k) add(ld_pos<DIM>(P + __ldg(&row[k])));
-    if (active) density_epilogue<T>(d, i, p, (double)dens - (double)comp);
+    if (active) density_epilogue<T, DIM>(d, i, p, (double)dens - (double)comp);
   }
 }
 
@@ -832,7 +832,10 @@ __global__ void k_pressure(Dev d) {
   const double dens = d.dens[i];
   const double press = p.csq * (d.pos[i].w * dens - p.rho0);
   d.press[i] = press;
-  write_record<T>(d, i, p, ti, dens, press);
+  if (p.dim == 3)
+    write_record<T, 3>(d, i, p, ti, dens, press);
+  else
+    write_record<T, 2>(d, i, p, ti, dens, press);
 }
 
 // Pair pass (kernel_vel_gradients.cu:15-662 and kernel_forces.cu:15-865 in one sweep),
@@ -896,7 +899,7 @@ constexpr int pair_min_blocks() {
 
 template <typename T, int DIM, int MODE, bool EXT>
 __global__ void __launch_bounds__(kPairWarps * 32, pair_min_blocks<T, DIM>()) k_pairs(Dev d) {
-  using Rec = typename RecOf<T>::type;
+  using Rec = typename RecFor<T, DIM>::type;
   using St = PairStage<Rec>;
   __shared__ int4 stage[kPairWarps][2][32 * St::kStride];
   const int w = threadIdx.x >> 5, lane = threadIdx.x & 31;
@@ -907,12 +910,13 @@ __global__ void __launch_bounds__(kPairWarps * 32, pair_min_blocks<T, DIM>()) k_
   const int is = active ? i : wbase;  // lanes past the end mirror a valid slot, compute nothing
 
   const Rec* __restrict__ rec = reinterpret_cast<const Rec*>(d.rec);
-  const BoxParams& p = d.box[box_of(d.tinfo[is])];
+  const int ti = d.tinfo[is];
+  const BoxParams& p = d.box[box_of(ti)];
   PairParams<T, DIM> pp;
   pp.load(p);
   const CollView cv{d.cs, d.ncoll};
   PairOwn<T, DIM> o;
-  load_own<T, DIM, MODE>(d, is, rec[is], o);
+  load_own<T, DIM, MODE>(d, is, ti, rec[is], o);
   PairAcc<T, DIM> acc;
   acc.zero();
   const int n = active ? min(d.nbr_cnt[i], d.cap) : 0;
@@ -927,6 +931,9 @@ __global__ void __launch_bounds__(kPairWarps * 32, pair_min_blocks<T, DIM>()) k_
   int4 nxt = n > 4 ? __ldg(&row[1]) : make_int4(-1, -1, -1, -1);
   int4* sb = &stage[w][0][0];
   int jc = n > 0 ? cur.x : -1;
+  // 2D records carry no type word: the neighbour's is read from the type array one
+  // position ahead, with its record's copy
+  int tc = DIM == 2 && jc >= 0 ? __ldg(&d.tinfo[jc]) : 0;
   stage_records<Rec>(sb, rec, jc, lane);
   cp_async_commit();
   for (int k = 0; k < nmax; ++k) {
@@ -938,6 +945,7 @@ __global__ void __launch_bounds__(kPairWarps * 32, pair_min_blocks<T, DIM>()) k_
     const int q = k1 & 3;
     const int jn = k1 < n ? (q == 0 ? cur.x : q == 1 ? cur.y : q == 2 ? cur.z : cur.w) : -1;
     if (k1 < nmax) stage_records<Rec>(sb + (k1 & 1) * 32 * St::kStride, rec, jn, lane);
+    const int tn = DIM == 2 && jn >= 0 ? __ldg(&d.tinfo[jn]) : 0;
     cp_async_commit();
     cp_async_wait_prev();  // position k has landed (this lane's copies) ...
     __syncwarp();          // ... and every other lane's
@@ -946,16 +954,22 @@ __global__ void __launch_bounds__(kPairWarps * 32, pair_min_blocks<T, DIM>()) k_
       if constexpr (sizeof(T) == 8) {
         // FP64: the neighbour's record is read in place, each field loaded where the pair
         // term uses it, which keeps the 128-byte record out of the register file
-        pair_term<T, DIM>(p, pp, cv, o, *reinterpret_cast<const Rec*>(src), acc);
+        const Rec& rj = *reinterpret_cast<const Rec*>(src);
+        int tj;
+        if constexpr (DIM == 3) tj = type_of(rj.tinfo); else tj = type_of(tc);
+        pair_term<T, DIM>(p, pp, cv, o, rj, tj, acc);
       } else {
         typename St::Slot rj;
 #pragma unroll
         for (int t = 0; t < St::kPieces; ++t) rj.v[t] = src[t];
-        pair_term<T, DIM>(p, pp, cv, o, rj.r, acc);
+        int tj;
+        if constexpr (DIM == 3) tj = type_of(rj.r.tinfo); else tj = type_of(tc);
+        pair_term<T, DIM>(p, pp, cv, o, rj.r, tj, acc);
       }
     }
     __syncwarp();  // buffer k & 1 is refilled at position k + 2
     jc = jn;
+    tc = tn;
   }
   if (active) pair_store<T, DIM, MODE, EXT>(d, i, p, o, acc);
 }
