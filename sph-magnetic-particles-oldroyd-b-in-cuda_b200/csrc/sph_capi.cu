@@ -550,7 +550,9 @@ sph_status sph_create_ensemble(int nboxes, const sph_input* inputs,
   d.ncoll = ncoll;
   d.nwallseg = nwall;
   d.Nlist_coll = nlist;
-  d.cap = o.nbr_capacity > 0 ? o.nbr_capacity : derived_capacity(c->boxes, c->dim);
+  // list rows hold a multiple of 8 entries: rows start 32-byte aligned and are read and
+  // written in aligned 16- and 32-byte groups
+  d.cap = o.nbr_capacity > 0 ? (o.nbr_capacity + 7) / 8 * 8 : derived_capacity(c->boxes, c->dim);
   c->key_bits = bits_for(std::max(Ctot, 2));
   const size_t Np = d.Npad;
   bool ok = true;

@@ -378,6 +378,10 @@ __global__ void __launch_bounds__(kListWarps * 32) k_build_lists(Dev d) {
   __shared__ __align__(16) float stage_x[kListWarps][32];
   __shared__ __align__(16) float stage_y[kListWarps][32];
   __shared__ __align__(16) float stage_z[kListWarps][32];
+  // each lane's pending list entries, one column per lane (conflict-free single-entry
+  // writes); a lane writes its row in groups of 8 entries, whole 32-byte sectors, instead
+  // of one scattered 4-byte store per entry
+  __shared__ int pending[kListWarps][8][32];
   const int w = threadIdx.x >> 5, lane = threadIdx.x & 31;
   const int sub = lane / TPC, gl = lane % TPC;  // group within the warp, lane within the group
   float* stx = &stage_x[w][sub * TPC];
@@ -432,6 +436,14 @@ __global__ void __launch_bounds__(kListWarps * 32) k_build_lists(Dev d) {
     const f32x2 cut22 = f2_pack(cut2, cut2);
     int* rowp = d.nbr + (size_t)(active ? i : 0) * cap;
     int cnt = 0;
+    int* pend = &pending[w][0][lane];
+    // entries base .. base + 7 of this lane's row from its pending column (base % 8 == 0:
+    // rows start 32-byte aligned, cap % 8 == 0)
+    auto flush8 = [&](int base) {
+      int4* dst = reinterpret_cast<int4*>(rowp + base);
+      dst[0] = make_int4(pend[0], pend[32], pend[64], pend[96]);
+      dst[1] = make_int4(pend[128], pend[160], pend[192], pend[224]);
+    };
     // the neighbour cells' candidate ranges: with a warp per cell, lane q loads those of
     // neighbour cell q up front (all 3^d loads in flight at once) and the loop takes them
     // by shuffle; a half-warp group loads them as it goes
@@ -524,12 +536,17 @@ __global__ void __launch_bounds__(kListWarps * 32) k_build_lists(Dev d) {
             while (hits) {
               const int q = __ffs(hits) - 1;
               hits &= hits - 1u;
-              if (cnt < cap) rowp[cnt] = c0 + q;
+              const int k8 = cnt & 7;
+              pend[k8 * 32] = c0 + q;
+              if (k8 == 7 && cnt < cap) flush8(cnt - 7);  // entries cnt - 7 .. cnt
               ++cnt;
             }
             __syncwarp();
           }
         }
+    // the last, partial group (the entries past cnt in it are never read); rows hold cap
+    // entries, cap a multiple of 8, so a group below cap lies wholly inside the row
+    if ((cnt & 7) != 0 && cnt < cap) flush8(cnt & ~7);
     if (active && !odd) {
       d.nbr_cnt[i] = cnt;
       maxcnt = max(maxcnt, cnt);
