@@ -382,6 +382,12 @@ __global__ void __launch_bounds__(kListWarps * 32) k_build_lists(Dev d) {
   // writes); a lane writes its row in groups of 8 entries, whole 32-byte sectors, instead
   // of one scattered 4-byte store per entry
   __shared__ int pending[kListWarps][8][32];
+  // each lane's hit mask per tested chunk, and the chunk's first slot per group; decoded in
+  // one loop per lane after the cells, so that the warp runs the busiest lane's total hit
+  // count rather than the busiest lane's count of every chunk
+  constexpr int kMaxCh = 32;
+  __shared__ unsigned hmask[kListWarps][kMaxCh][32];
+  __shared__ int hbase[kListWarps][kMaxCh][2];
   const int w = threadIdx.x >> 5, lane = threadIdx.x & 31;
   const int sub = lane / TPC, gl = lane % TPC;  // group within the warp, lane within the group
   float* stx = &stage_x[w][sub * TPC];
@@ -443,6 +449,26 @@ __global__ void __launch_bounds__(kListWarps * 32) k_build_lists(Dev d) {
       int4* dst = reinterpret_cast<int4*>(rowp + base);
       dst[0] = make_int4(pend[0], pend[32], pend[64], pend[96]);
       dst[1] = make_int4(pend[128], pend[160], pend[192], pend[224]);
+    };
+    int nmask = 0;  // chunks recorded since the last decode (warp-uniform)
+    // this lane's recorded hits, chunk by chunk and bit by bit (divergent, no warp sync)
+    auto decode = [&]() {
+      // one flat loop: an iteration either moves to this lane's next chunk or appends one
+      // hit, so lanes run independently and the warp runs the busiest lane's total
+      int m = 0;
+      unsigned mk = nmask > 0 ? hmask[w][0][lane] : 0u;
+      while (m < nmask) {
+        if (mk == 0u) {
+          if (++m < nmask) mk = hmask[w][m][lane];
+          continue;
+        }
+        const int q = __ffs(mk) - 1;
+        mk &= mk - 1u;
+        const int k8 = cnt & 7;
+        pend[k8 * 32] = hbase[w][m][sub] + q;
+        if (k8 == 7 && cnt < cap) flush8(cnt - 7);  // entries cnt - 7 .. cnt
+        ++cnt;
+      }
     };
     // the neighbour cells' candidate ranges: with a warp per cell, lane q loads those of
     // neighbour cell q up front (all 3^d loads in flight at once) and the loop takes them
@@ -532,18 +558,20 @@ __global__ void __launch_bounds__(kListWarps * 32) k_build_lists(Dev d) {
               hits = m > 0 ? __brev(hits) >> (32 - m) : 0u;
               if (TPC == 16) hits &= (listed && n > 0) ? (0xFFFFFFFFu >> (32 - n)) : 0u;
             }
-            // append in candidate order to the particle's own list row
-            while (hits) {
-              const int q = __ffs(hits) - 1;
-              hits &= hits - 1u;
-              const int k8 = cnt & 7;
-              pend[k8 * 32] = c0 + q;
-              if (k8 == 7 && cnt < cap) flush8(cnt - 7);  // entries cnt - 7 .. cnt
-              ++cnt;
+            // recorded for the decode after the cells (candidate order is kept)
+            hmask[w][nmask][lane] = hits;
+            if (gl == 0) hbase[w][nmask][sub] = c0;
+            if (++nmask == kMaxCh) {
+              __syncwarp();
+              decode();
+              nmask = 0;
             }
             __syncwarp();
           }
         }
+    __syncwarp();
+    decode();
+    __syncwarp();  // the mask table is refilled by the next round
     // the last, partial group (the entries past cnt in it are never read); rows hold cap
     // entries, cap a multiple of 8, so a group below cap lies wholly inside the row
     if ((cnt & 7) != 0 && cnt < cap) flush8(cnt & ~7);
