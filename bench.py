@@ -73,7 +73,7 @@ B_ALG_PAIRS = {"fp64": (6 + 6 + 1 + 1 + 6 + 1 + 3 + 6) * 8 + 4,
 # FP64 floating-point operations per particle of one launch of the FP64 pair kernel, counted
 # by ncu on the 96^3 case of this workload (same lattice, same neighbours per particle):
 # DADD + DMUL + 2 DFMA thread instructions / particles (profiles/k_pairs_couette96_fp64.md).
-FP64_PAIR_FLOP = 11842.3
+FP64_PAIR_FLOP = 11549.4
 # FP64 peak of the B200: 148 SMs x 64 FP64 FMA lanes (ncu's dfma peak_sustained, 9,472 per
 # cycle) x 2 FLOP x the SM clock.
 FP64_LANES = 9472
@@ -597,7 +597,7 @@ def main():
     ap.add_argument("--e2e-steps", type=int, default=20)
     ap.add_argument("--pairs-traffic", type=float, default=None,
                     help="ncu DRAM bytes per k_pairs launch (default: the FP64 capture at "
-                         "96^3, 788.8 MB, scaled by particle count to the benchmark)")
+                         "96^3, 786.6 MB, scaled by particle count to the benchmark)")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-autotune", action="store_true",
                     help="keep the default launch geometry (profiling runs: no tuning launches)")
@@ -607,7 +607,7 @@ def main():
     if args.pairs_traffic is None and args.lattice == 128 and args.precision in (None, "fp64"):
         # dram__bytes_read.sum + dram__bytes_write.sum of one k_pairs launch at 96^3
         # (940,032 particles), scaled to the 2,195,456 particles of the benchmark
-        args.pairs_traffic = (724.24448e6 + 64.03584e6) * 2195456 / 940032
+        args.pairs_traffic = (722.4832e6 + 64.10752e6) * 2195456 / 940032
     if args.precision is None:
         args.precision = "mixed" if args.workload == "sweep" else "fp64"
     if args.lattice != 128:
