@@ -118,6 +118,30 @@ def test_fp64_engine_matches_oracle_after_n_steps(name, workdir):
     o.close()
 
 
+@pytest.mark.parametrize("precision", ["fp64", "mixed"])
+def test_dense_cells_match_oracle(precision, workdir):
+    """A walled 3D box at overlap 4: cells of 64 particles, so the list build takes two
+    rounds per cell and more chunks per neighbourhood walk than its mask table holds (the
+    table is decoded part-way).  Against the FP64 oracle after 3 steps, cells bit-exact."""
+    inp = os.path.join(workdir, "input")
+    sph_input.write_input(inp, N=(24, 24, 24), L=(1.0, 1.0, 1.0), dim=3, overlap=4.0, wall=1,
+                          Vwall_bottom=-0.4, Vwall_top=0.4, dt=2e-5)
+    e = sph_b200.System(inp, precision=precision)
+    o = oracle.Oracle(inp)
+    o.run(0)
+    e.step(0)
+    o.run(3)
+    e.step(3)
+    e.synchronize()
+    tol = 1e-10 if precision == "fp64" else dict(MIXED_TOL)
+    compare_state(e, o, tol, "dense step3")
+    cells = e.export_cells()
+    for k in INTS:
+        assert np.array_equal(cells[k], o.ifield(k)), k
+    e.close()
+    o.close()
+
+
 @pytest.mark.parametrize("name", list(mg.CASES))
 def test_mixed_engine_matches_oracle(name, workdir):
     e, o = open_case(name, workdir, precision="mixed")
