@@ -201,9 +201,12 @@ int ph_search(sph_ctx* c) {
   return 0;
 }
 
-int ph_forces(sph_ctx* c) {
+// fold: the fused pair pass also applies the step's second half-kick to fluid particles
+// (the step graph); the method-by-method path keeps V_Verlet_step2 separate
+int ph_forces(sph_ctx* c, bool fold = false) {
   Launch L = launcher(c);
   L.d.gradv = nullptr;  // the fused pass keeps the gradient in registers
+  L.d.fold_vv2 = fold ? 1 : 0;
   bool ext = false;
   for (const HostBox& hb : c->boxes) ext = ext || hb.p.ext_force_type != 0;
   if (launch_density_dim(L, c->dim)) return 1;
@@ -225,9 +228,9 @@ int ph_vv1(sph_ctx* c) {
   return 0;
 }
 
-int ph_vv2(sph_ctx* c) {
+int ph_vv2(sph_ctx* c, bool folded = false) {
   Launch L = launcher(c);
-  if (launch_vv2(L) || launch_count_step(L)) return 1;
+  if (launch_vv2(L, !folded) || launch_count_step(L)) return 1;
   return 0;
 }
 
@@ -235,7 +238,7 @@ int ph_vv2(sph_ctx* c) {
 int ph_step(sph_ctx* c) {
   if (ph_vv1(c) || ph_search(c)) return 1;
   if (launch_advance_time(launcher(c), 0)) return 1;
-  if (ph_forces(c) || ph_vv2(c)) return 1;
+  if (ph_forces(c, true) || ph_vv2(c, true)) return 1;
   c->forces_live = true;
   return 0;
 }
@@ -1002,6 +1005,7 @@ sph_status sph_profile_phases(sph_ctx* c, int nsteps, double* ms) {
     cudaEventRecord(ev[6], c->stream);
     Launch Lf = L;
     Lf.d.gradv = nullptr;
+    Lf.d.fold_vv2 = 1;  // as in the step graph: fluid half-kick inside the pair pass
     bad |= launch_density_dim(Lf, c->dim);
     cudaEventRecord(ev[7], c->stream);
     bad |= launch_pairs_dim(Lf, c->dim, kPairFused, ext ? 1 : 0);
@@ -1010,7 +1014,7 @@ sph_status sph_profile_phases(sph_ctx* c, int nsteps, double* ms) {
     cudaEventRecord(ev[9], c->stream);
     bad |= launch_colloid_forces(Lf, pairs ? 1 : 0);
     cudaEventRecord(ev[10], c->stream);
-    bad |= launch_vv2(L) | launch_count_step(L);
+    bad |= launch_vv2(L, false) | launch_count_step(L);
     cudaEventRecord(ev[11], c->stream);
     cudaEventSynchronize(ev[11]);
     for (int k = 0; k < SPH_NUM_PHASES; ++k) {

@@ -568,6 +568,18 @@ __device__ __forceinline__ void pair_term(const BoxParams& p, const PairParams<T
   }
 }
 
+// Second half-kick of a fluid particle's velocity, v += (dt / 2) f / m
+// (kernel_move_sys_VV_part2.cu:13-58), as explicit fused multiply-adds so that the step's
+// fused form and the standalone V_Verlet_step2 give the same bits.
+template <int DIM>
+__device__ __forceinline__ void vv2_fluid(const BoxParams& p, double mass, double fx, double fy,
+                                          double fz, double4& v) {
+  const double hm = 0.5 * p.dt / mass;
+  v.x = __fma_rn(hm, fx, v.x);
+  v.y = __fma_rn(hm, fy, v.y);
+  if (DIM == 3) v.z = __fma_rn(hm, fz, v.z);
+}
+
 // stored gradient, forces with the body force, and dc/dt of particle i
 template <typename T, int DIM, int MODE, bool EXT>
 __device__ __forceinline__ void pair_store(const Dev& d, int i, const BoxParams& p,
@@ -618,19 +630,20 @@ __device__ __forceinline__ void pair_store(const Dev& d, int i, const BoxParams&
   if (MODE == kPairFused && o.fluid) {
     // dc/dt = c.g + (c.g)^T + (I - c)/tau  (kernel_dcdt.cu:76-102)
     const double tinv = 1.0 / p.tau;
+    double dc[6];
     const double cxx = d.conf[i], cxy = d.conf[Np2 + i], cyy = d.conf[2 * Np2 + i];
     if (DIM == 2) {
       const double gxx = acc.grad(0, 0), gxy = acc.grad(0, 1), gyx = acc.grad(1, 0),
                    gyy = acc.grad(1, 1);
       const double Axx = cxx * gxx + cxy * gyx, Axy = cxx * gxy + cxy * gyy;
       const double Ayx = cxy * gxx + cyy * gyx, Ayy = cxy * gxy + cyy * gyy;
-      d.dcdt[i] = 2.0 * Axx + tinv * (1.0 - cxx);
-      d.dcdt[Np2 + i] = Axy + Ayx - tinv * cxy;
-      d.dcdt[2 * Np2 + i] = 2.0 * Ayy + tinv * (1.0 - cyy);
+      dc[0] = 2.0 * Axx + tinv * (1.0 - cxx);
+      dc[1] = Axy + Ayx - tinv * cxy;
+      dc[2] = 2.0 * Ayy + tinv * (1.0 - cyy);
       // the z components stay zero in 2D
-      d.dcdt[3 * Np2 + i] = 0.0;
-      d.dcdt[4 * Np2 + i] = 0.0;
-      d.dcdt[5 * Np2 + i] = 0.0;
+      dc[3] = 0.0;
+      dc[4] = 0.0;
+      dc[5] = 0.0;
     } else {
       const double cxz = d.conf[3 * Np2 + i], cyz = d.conf[4 * Np2 + i], czz = d.conf[5 * Np2 + i];
       const double gxx = acc.grad(0, 0), gxy = acc.grad(0, 1), gxz = acc.grad(0, DIM - 1);
@@ -646,12 +659,24 @@ __device__ __forceinline__ void pair_store(const Dev& d, int i, const BoxParams&
       const double Azx = cxz * gxx + cyz * gyx + czz * gzx;
       const double Azy = cxz * gxy + cyz * gyy + czz * gzy;
       const double Azz = cxz * gxz + cyz * gyz + czz * gzz;
-      d.dcdt[i] = 2.0 * Axx + tinv * (1.0 - cxx);
-      d.dcdt[Np2 + i] = Axy + Ayx - tinv * cxy;
-      d.dcdt[2 * Np2 + i] = 2.0 * Ayy + tinv * (1.0 - cyy);
-      d.dcdt[3 * Np2 + i] = Axz + Azx - tinv * cxz;
-      d.dcdt[4 * Np2 + i] = Ayz + Azy - tinv * cyz;
-      d.dcdt[5 * Np2 + i] = 2.0 * Azz + tinv * (1.0 - czz);
+      dc[0] = 2.0 * Axx + tinv * (1.0 - cxx);
+      dc[1] = Axy + Ayx - tinv * cxy;
+      dc[2] = 2.0 * Ayy + tinv * (1.0 - cyy);
+      dc[3] = Axz + Azx - tinv * cxz;
+      dc[4] = Ayz + Azy - tinv * cyz;
+      dc[5] = 2.0 * Azz + tinv * (1.0 - czz);
+    }
+#pragma unroll
+    for (int q = 0; q < 6; ++q) d.dcdt[q * Np2 + i] = dc[q];
+    if (d.fold_vv2) {
+      // the step's second half-kick of this fluid particle (kernel_move_sys_VV_part2.cu:13-58),
+      // the same operations as vv2_fluid, on the force and rate just stored
+      double4 v = d.vel[i];
+      vv2_fluid<DIM>(p, d.pos[i].w, fx, fy, fz, v);
+      d.vel[i] = v;
+#pragma unroll
+      for (int q = 0; q < (DIM == 3 ? 6 : 3); ++q)
+        d.conf[q * Np2 + i] = __fma_rn(0.5 * p.dt, dc[q], d.conf[q * Np2 + i]);
     }
   }
 }

@@ -191,6 +191,7 @@ struct Dev {
   unsigned* status;
   int* err_info;       // [0] first bad slot, [1] largest neighbour count seen
   int grad_all;        // fused pair pass: velocity gradient of every particle, not only fluid
+  int fold_vv2;        // fused pair pass: also the step's second half-kick of fluid particles
 };
 
 // Colloid state layout in Dev::cs (each row ncoll long).
@@ -224,7 +225,7 @@ inline int& last_launch_error() {
 
 int launch_vv1_particles(const Launch& L);
 int launch_vv1_colloids(const Launch& L);
-int launch_vv2(const Launch& L);
+int launch_vv2(const Launch& L, bool particles = true);
 int launch_hash(const Launch& L);
 int launch_reorder(const Launch& L, bool permute_forces);
 int launch_build_lists_dim(const Launch& L, int dim);

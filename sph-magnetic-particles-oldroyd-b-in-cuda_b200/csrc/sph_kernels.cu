@@ -74,20 +74,14 @@ __global__ void k_vv2_particles(Dev d) {
   if (type_of(ti) != 0) return;
   const BoxParams& p = d.box[box_of(ti)];
   const int Np = d.Npad;
-  double h = 0.5 * p.dt;
-  double hm = h / d.pos[i].w;
+  const double h = 0.5 * p.dt;
   double4 v = d.vel[i];
-  v.x = v.x + hm * d.f[i];
-  v.y = v.y + hm * d.f[Np + i];
-  d.conf[i] = d.conf[i] + h * d.dcdt[i];
-  d.conf[Np + i] = d.conf[Np + i] + h * d.dcdt[Np + i];
-  d.conf[2 * Np + i] = d.conf[2 * Np + i] + h * d.dcdt[2 * Np + i];
-  if (p.dim == 3) {
-    v.z = v.z + hm * d.f[2 * Np + i];
-    d.conf[3 * Np + i] = d.conf[3 * Np + i] + h * d.dcdt[3 * Np + i];
-    d.conf[4 * Np + i] = d.conf[4 * Np + i] + h * d.dcdt[4 * Np + i];
-    d.conf[5 * Np + i] = d.conf[5 * Np + i] + h * d.dcdt[5 * Np + i];
-  }
+  const int nc = p.dim == 3 ? 6 : 3;
+  if (p.dim == 3)
+    vv2_fluid<3>(p, d.pos[i].w, d.f[i], d.f[Np + i], d.f[2 * Np + i], v);
+  else
+    vv2_fluid<2>(p, d.pos[i].w, d.f[i], d.f[Np + i], 0.0, v);
+  for (int q = 0; q < nc; ++q) d.conf[q * Np + i] = __fma_rn(h, d.dcdt[q * Np + i], d.conf[q * Np + i]);
   d.vel[i] = v;
 }
 
@@ -1520,8 +1514,8 @@ int launch_vv1_colloids(const Launch& L) {
   return check(L);
 }
 
-int launch_vv2(const Launch& L) {
-  if (L.d.Ntot > 0) {
+int launch_vv2(const Launch& L, bool particles) {
+  if (particles && L.d.Ntot > 0) {
     k_vv2_particles<<<blocks(L.d.Ntot, kT), kT, 0, S(L)>>>(L.d);
     if (check(L)) return 1;
   }
