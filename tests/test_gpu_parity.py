@@ -343,6 +343,33 @@ def test_graph_and_direct_paths_agree(workdir):
         assert np.array_equal(a.field(f), b.field(f)), f
 
 
+@pytest.mark.parametrize("precision", ["fp64", "mixed"])
+@pytest.mark.parametrize("name", ["kolmogorov2d", "couette2d", "couette3d"])
+def test_step_graph_equals_method_sequence(name, precision, workdir):
+    """The step graph, whose pair pass also applies the fluid particles' second half-kick,
+    against the class_system call sequence of main.cu:358-467 (V_Verlet_step1,
+    neighbours_search, calculate_forces, V_Verlet_step2): the same bits."""
+    a, _ = open_case(name, workdir, precision=precision)
+    b, _ = open_case(name, workdir, precision=precision)
+    a.step(4)
+    b.initial_forces()
+    for _ in range(4):
+        b.V_Verlet_step1()
+        b.neighbours_search()
+        b.calculate_forces()
+        b.V_Verlet_step2()
+    a.synchronize()
+    b.synchronize()
+    fields = ["x", "y", "vx", "vy", "fx", "fy", "dens", "cxx", "cxy", "cyy"]
+    if a.info()["dim"] == 3:
+        fields += ["z", "vz", "cxz", "cyz", "czz"]
+    for f in fields:
+        assert np.array_equal(a.field(f), b.field(f)), f
+    assert np.array_equal(a.wall_forces(), b.wall_forces())
+    a.close()
+    b.close()
+
+
 def test_ensemble_equals_single_boxes(workdir):
     """Boxes of different sizes and parameters in one context give, box by box, the same
     bits as each box run alone."""
