@@ -449,7 +449,104 @@ __device__ __forceinline__ void load_own(const Dev& d, int i, int ti, const Rec&
   o.do_force = MODE != kPairGradvAll;
 }
 
-// tj: the neighbour's particle type
+// Separation r = x_i - x_j under the minimum image; returns |r|^2.
+template <typename T, int DIM, typename Rec>
+__device__ __forceinline__ T pair_sep(const PairParams<T, DIM>& pp, int wall,
+                                      const PairOwn<T, DIM>& o, const Rec& rj, T r[3]) {
+  r[0] = o.x - (T)rj.x;
+  r[1] = o.y - (T)rj.y;
+  r[2] = DIM == 3 ? o.z - (T)rec_z<DIM>(rj) : T(0);
+  min_image<T, DIM>(r[0], r[1], r[2], pp.L, pp.h, wall);
+  return DIM == 3 ? r[0] * r[0] + r[1] * r[1] + r[2] * r[2] : r[0] * r[0] + r[1] * r[1];
+}
+
+// 1/|r|, the kernel slope gw = dW/dr at |r| and the unit vector e = r / |r|.
+template <typename T, int DIM>
+struct PairRadial {
+  T rinv, gw, e[3];
+  __device__ __forceinline__ void eval(const PairParams<T, DIM>& pp, T r2, const T r[3]) {
+    rinv = rsqrt(r2);  // r and 1/r from one reciprocal square root
+    const T rr = r2 * rinv;
+    gw = sph_gradw<T>(rr, pp.rcut_inv, pp.c_gradw);
+    e[0] = r[0] * rinv;
+    e[1] = r[1] * rinv;
+    e[2] = DIM == 3 ? r[2] * rinv : T(0);
+  }
+};
+
+// Velocity-gradient term, g_ac += -(1/d_i) gw e_a v_c (kernel_vel_gradients.cu:334-337,
+// 632-640).
+template <typename T, int DIM>
+__device__ __forceinline__ void pair_grad_add(const PairOwn<T, DIM>& o, const PairRadial<T, DIM>& g,
+                                              const T v[3], PairAcc<T, DIM>& acc) {
+  const T s = -o.invd * g.gw;
+#pragma unroll
+  for (int a = 0; a < DIM; ++a) {
+    const T se = s * g.e[a];
+#pragma unroll
+    for (int c = 0; c < DIM; ++c) {
+      if constexpr (PairAcc<T, DIM>::kComp)
+        kahan_add(acc.g[a][c], acc.cg[a][c], se * v[c]);
+      else
+        acc.g[a][c] += se * v[c];
+    }
+  }
+}
+
+// Force term from the partners' stress terms Pi, Pj (P/d^2 - nkT c/d^2) and inverse
+// densities di, dj: the reversible part -gw (Pi + Pj).e and the viscous part
+// a gw/(di dj r) v + b gw/(di dj r) (e.v) e (kernel_forces.cu:426-440, 826-850).
+template <typename T, int DIM>
+__device__ __forceinline__ void pair_force_add(const PairParams<T, DIM>& pp,
+                                               const PairRadial<T, DIM>& g, const T v[3],
+                                               const T Pi[6], const T Pj[6], T di, T dj,
+                                               PairAcc<T, DIM>& acc) {
+  const T gw = g.gw;
+  const T* e = g.e;
+  const T aux = gw * di * dj * g.rinv;
+  const T aux1 = pp.a * aux;
+  if constexpr (PairAcc<T, DIM>::kComp) {
+    // the pair's force as one term per component, then one compensated add
+    const T axx = -gw * (Pi[0] + Pj[0]);
+    const T axy = -gw * (Pi[1] + Pj[1]);
+    const T ayy = -gw * (Pi[2] + Pj[2]);
+    T ev = e[0] * v[0] + e[1] * v[1];
+    T t0 = axx * e[0] + axy * e[1], t1 = axy * e[0] + ayy * e[1], t2 = T(0);
+    if (DIM == 3) {
+      const T axz = -gw * (Pi[3] + Pj[3]);
+      const T ayz = -gw * (Pi[4] + Pj[4]);
+      const T azz = -gw * (Pi[5] + Pj[5]);
+      ev += e[2] * v[2];
+      t0 += axz * e[2];
+      t1 += ayz * e[2];
+      t2 = axz * e[0] + ayz * e[1] + azz * e[2];
+    }
+    const T aux2 = pp.b * aux * ev;
+    kahan_add(acc.f[0], acc.cf[0], t0 + (aux1 * v[0] + aux2 * e[0]));
+    kahan_add(acc.f[1], acc.cf[1], t1 + (aux1 * v[1] + aux2 * e[1]));
+    if (DIM == 3) kahan_add(acc.f[2], acc.cf[2], t2 + (aux1 * v[2] + aux2 * e[2]));
+  } else {
+    // -gw (Pi + Pj).e and the viscous terms folded into the sums by fused multiply-adds
+    const T ngw = -gw;
+    T ev = e[0] * v[0] + e[1] * v[1];
+    T t0 = (Pi[0] + Pj[0]) * e[0] + (Pi[1] + Pj[1]) * e[1];
+    T t1 = (Pi[1] + Pj[1]) * e[0] + (Pi[2] + Pj[2]) * e[1];
+    T t2 = T(0);
+    if (DIM == 3) {
+      const T sxz = Pi[3] + Pj[3], syz = Pi[4] + Pj[4];
+      ev += e[2] * v[2];
+      t0 += sxz * e[2];
+      t1 += syz * e[2];
+      t2 = sxz * e[0] + syz * e[1] + (Pi[5] + Pj[5]) * e[2];
+    }
+    const T aux2 = pp.b * aux * ev;
+    acc.f[0] = fma(aux2, e[0], fma(aux1, v[0], fma(ngw, t0, acc.f[0])));
+    acc.f[1] = fma(aux2, e[1], fma(aux1, v[1], fma(ngw, t1, acc.f[1])));
+    if (DIM == 3) acc.f[2] = fma(aux2, e[2], fma(aux1, v[2], fma(ngw, t2, acc.f[2])));
+  }
+}
+
+// One (i, j) pair.  tj: the neighbour's particle type.
 template <typename T, int DIM, typename Rec>
 __device__ __forceinline__ void pair_term(const BoxParams& p, const PairParams<T, DIM>& pp,
                                           const CollView& cv, const PairOwn<T, DIM>& o,
@@ -459,9 +556,8 @@ __device__ __forceinline__ void pair_term(const BoxParams& p, const PairParams<T
   const bool pair_grad = o.do_grad && !(o.t == tj && !o.fluid);
   const bool pair_force = o.do_force && (o.fluid || fluid_j);
   if (!pair_grad && !pair_force) return;
-  T r[3] = {o.x - (T)rj.x, o.y - (T)rj.y, DIM == 3 ? o.z - (T)rec_z<DIM>(rj) : T(0)};
-  min_image<T, DIM>(r[0], r[1], r[2], pp.L, pp.h, p.wall);
-  const T r2 = DIM == 3 ? r[0] * r[0] + r[1] * r[1] + r[2] * r[2] : r[0] * r[0] + r[1] * r[1];
+  T r[3];
+  const T r2 = pair_sep<T, DIM>(pp, p.wall, o, rj, r);
   if (!(r2 < pp.rcutsq)) return;
   const T vj[3] = {(T)rj.vx, (T)rj.vy, (T)rec_vz<DIM>(rj)};
   T v[3];
@@ -475,24 +571,9 @@ __device__ __forceinline__ void pair_term(const BoxParams& p, const PairParams<T
     ghost_solid_i<T, DIM>(p, cv, o.t, p.coll0, o.y, (T)rj.x, (T)rj.y, (T)rec_z<DIM>(rj), vj, r, pp.L,
                           pp.h, v);
   }
-  const T rinv = rsqrt(r2);  // r and 1/r from one reciprocal square root
-  const T rr = r2 * rinv;
-  const T gw = sph_gradw<T>(rr, pp.rcut_inv, pp.c_gradw);
-  const T e[3] = {r[0] * rinv, r[1] * rinv, DIM == 3 ? r[2] * rinv : T(0)};
-  if (pair_grad) {
-    const T s = -o.invd * gw;
-#pragma unroll
-    for (int a = 0; a < DIM; ++a) {
-      const T se = s * e[a];
-#pragma unroll
-      for (int c = 0; c < DIM; ++c) {
-        if constexpr (PairAcc<T, DIM>::kComp)
-          kahan_add(acc.g[a][c], acc.cg[a][c], se * v[c]);
-        else
-          acc.g[a][c] += se * v[c];
-      }
-    }
-  }
+  PairRadial<T, DIM> g;
+  g.eval(pp, r2, r);
+  if (pair_grad) pair_grad_add<T, DIM>(o, g, v, acc);
   if (pair_force) {
     T Pi[6], Pj[6], di, dj;
     if (o.fluid && fluid_j) {
@@ -524,46 +605,42 @@ __device__ __forceinline__ void pair_term(const BoxParams& p, const PairParams<T
       di = rj.invd;
       dj = rj.invd;
     }
-    const T axx = -gw * (Pi[0] + Pj[0]);
-    const T axy = -gw * (Pi[1] + Pj[1]);
-    const T ayy = -gw * (Pi[2] + Pj[2]);
-    const T aux = gw * di * dj * rinv;
-    const T aux1 = pp.a * aux;
-    if constexpr (PairAcc<T, DIM>::kComp) {
-      // the pair's force as one term per component, then one compensated add
-      T ev = e[0] * v[0] + e[1] * v[1];
-      T t0 = axx * e[0] + axy * e[1], t1 = axy * e[0] + ayy * e[1], t2 = T(0);
-      if (DIM == 3) {
-        const T axz = -gw * (Pi[3] + Pj[3]);
-        const T ayz = -gw * (Pi[4] + Pj[4]);
-        const T azz = -gw * (Pi[5] + Pj[5]);
-        ev += e[2] * v[2];
-        t0 += axz * e[2];
-        t1 += ayz * e[2];
-        t2 = axz * e[0] + ayz * e[1] + azz * e[2];
-      }
-      const T aux2 = pp.b * aux * ev;
-      kahan_add(acc.f[0], acc.cf[0], t0 + (aux1 * v[0] + aux2 * e[0]));
-      kahan_add(acc.f[1], acc.cf[1], t1 + (aux1 * v[1] + aux2 * e[1]));
-      if (DIM == 3) kahan_add(acc.f[2], acc.cf[2], t2 + (aux1 * v[2] + aux2 * e[2]));
-    } else {
-      // -gw (Pi + Pj).e and the viscous terms folded into the sums by fused multiply-adds
-      const T ngw = -gw;
-      T ev = e[0] * v[0] + e[1] * v[1];
-      T t0 = (Pi[0] + Pj[0]) * e[0] + (Pi[1] + Pj[1]) * e[1];
-      T t1 = (Pi[1] + Pj[1]) * e[0] + (Pi[2] + Pj[2]) * e[1];
-      T t2 = T(0);
-      if (DIM == 3) {
-        const T sxz = Pi[3] + Pj[3], syz = Pi[4] + Pj[4];
-        ev += e[2] * v[2];
-        t0 += sxz * e[2];
-        t1 += syz * e[2];
-        t2 = sxz * e[0] + syz * e[1] + (Pi[5] + Pj[5]) * e[2];
-      }
-      const T aux2 = pp.b * aux * ev;
-      acc.f[0] = fma(aux2, e[0], fma(aux1, v[0], fma(ngw, t0, acc.f[0])));
-      acc.f[1] = fma(aux2, e[1], fma(aux1, v[1], fma(ngw, t1, acc.f[1])));
-      if (DIM == 3) acc.f[2] = fma(aux2, e[2], fma(aux1, v[2], fma(ngw, t2, acc.f[2])));
+    pair_force_add<T, DIM>(pp, g, v, Pi, Pj, di, dj, acc);
+  }
+}
+
+// Two list positions of a fluid particle whose partners there are fluid particles (or
+// absent), evaluated side by side.  Each term is pair_term's fluid-fluid term; both are
+// computed before either is added, so that their dependency chains overlap, and the sums
+// take them in list order.  va, vb: the position holds a partner; an absent position is
+// computed from whatever its staging slot holds and not added.
+template <typename T, int DIM, typename Rec>
+__device__ __forceinline__ void pair_fluid_x2(const BoxParams& p, const PairParams<T, DIM>& pp,
+                                              const PairOwn<T, DIM>& o, const Rec& ra, bool va,
+                                              const Rec& rb, bool vb, PairAcc<T, DIM>& acc) {
+  T r[2][3], v[2][3];
+  PairRadial<T, DIM> g[2];
+  bool in[2];
+  const Rec* rj[2] = {&ra, &rb};
+  const bool valid[2] = {va, vb};
+#pragma unroll
+  for (int u = 0; u < 2; ++u) {
+    const T r2 = pair_sep<T, DIM>(pp, p.wall, o, *rj[u], r[u]);
+    in[u] = valid[u] && r2 < pp.rcutsq;
+    v[u][0] = o.v[0] - (T)rj[u]->vx;
+    v[u][1] = o.v[1] - (T)rj[u]->vy;
+    v[u][2] = o.v[2] - (T)rec_vz<DIM>(*rj[u]);
+    g[u].eval(pp, r2, r[u]);
+  }
+#pragma unroll
+  for (int u = 0; u < 2; ++u) {
+    if (!in[u]) continue;
+    if (o.do_grad) pair_grad_add<T, DIM>(o, g[u], v[u], acc);
+    if (o.do_force) {
+      T Pj[6];
+#pragma unroll
+      for (int q = 0; q < 6; ++q) Pj[q] = rec_P<DIM>(*rj[u], q);
+      pair_force_add<T, DIM>(pp, g[u], v[u], o.P, Pj, o.invd, (T)rj[u]->invd, acc);
     }
   }
 }

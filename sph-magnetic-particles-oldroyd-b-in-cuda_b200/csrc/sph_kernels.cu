@@ -885,16 +885,32 @@ __global__ void k_pressure(Dev d) {
 // per instruction, that is 32 separate cache lines per instruction.  Instead the warp
 // copies the 32 records into shared memory cooperatively: kPieces consecutive lanes move
 // the pieces of one record, so one copy instruction covers whole lines of 32 / kPieces
-// records.  The copies for position k + 1 (cp.async, double buffer) are in flight while
-// position k is evaluated.  Each lane then reads its record from shared memory with
-// 16-byte loads (row stride padded by one piece: conflict-free).
-constexpr int kPairWarps = 4;
+// records.  The copies for the next position (or the next two) are in flight (cp.async,
+// double buffer) while the current ones are evaluated.  Each lane then reads its records
+// from shared memory (row stride padded by one piece: conflict-free).
+//
+// Launch shape of the pair pass per precision and dimension, as measured on B200:
+//  - kILP: list positions evaluated per step.  Two side by side (pair_fluid_x2) hide the
+//    latency of the float 3D and FP64 2D terms; the FP64 3D pass, held to 12 warps per SM
+//    by its 168 registers, and the float 2D pass run faster one position at a time.
+//  - kWarps: warps per block; kMinBlocks: resident blocks per SM the register allocation
+//    is held to (FP64 3D: 168 registers, which its working set fits without spilling; the
+//    others 128).
+template <typename T, int DIM>
+struct PairShape {
+  using Rec = typename RecFor<T, DIM>::type;
+  static constexpr bool kF64 = sizeof(T) == 8;
+  static constexpr int kILP = (kF64 && DIM == 3) || (!kF64 && DIM == 2) ? 1 : 2;
+  static constexpr int kWarps = 4;
+  static constexpr int kMinBlocks = kILP == 1 ? 3 : 4;
+};
 
 template <typename Rec>
 struct PairStage {
   static constexpr int kPieces = (int)(sizeof(Rec) / 16);  // 16-byte pieces per record
   static constexpr int kStride = kPieces + 1;               // padded row, in pieces
   static constexpr int kPerCopy = 32 / kPieces;             // records per copy instruction
+  static constexpr int kRows = 32 * kStride;                // one position, in pieces
   union Slot {
     int4 v[kPieces];
     Rec r;
@@ -928,21 +944,153 @@ __device__ __forceinline__ void stage_records(int4* buf, const Rec* __restrict__
   }
 }
 
-// Resident blocks per SM the register allocation is held to: 3 (at most 168 registers) for
-// the FP64 3D pass, whose working set spills at 4; 4 for the FP64 2D pass, which fits in
-// 128 registers; the float passes fit 4 blocks either way.
+// A lane's view of one staged record: FP64 records are read in place, each field loaded
+// from shared memory where the pair term uses it, which keeps the 128-byte record out of
+// the register file; float records are copied into registers.
+template <typename T, typename Rec>
+struct StagedRec {
+  const Rec& r;
+  __device__ __forceinline__ explicit StagedRec(const int4* src)
+      : r(*reinterpret_cast<const Rec*>(src)) {}
+};
+template <typename Rec>
+struct StagedRec<float, Rec> {
+  Rec r;
+  __device__ __forceinline__ explicit StagedRec(const int4* src) {
+    typename PairStage<Rec>::Slot s;
+#pragma unroll
+    for (int t = 0; t < PairStage<Rec>::kPieces; ++t) s.v[t] = src[t];
+    r = s.r;
+  }
+};
+
+// Everything a lane's walk over its list needs.
 template <typename T, int DIM>
-constexpr int pair_min_blocks() {
-  return sizeof(T) == 8 && DIM == 2 ? 4 : 3;
+struct PairWalk {
+  using Rec = typename RecFor<T, DIM>::type;
+  const Dev& d;
+  const Rec* __restrict__ rec;
+  const int4* __restrict__ row;  // the lane's list row, four indices per load
+  int4* sb;                      // the warp's staging rows
+  int lane, i, n, nmax;
+  const BoxParams& p;
+  const PairParams<T, DIM>& pp;
+  const CollView& cv;
+  const PairOwn<T, DIM>& o;
+};
+
+// One position per step: the copies for position k + 1 are in flight while k is evaluated.
+template <typename T, int DIM>
+__device__ __forceinline__ void pair_walk1(const PairWalk<T, DIM>& W, PairAcc<T, DIM>& acc) {
+  using Rec = typename RecFor<T, DIM>::type;
+  using St = PairStage<Rec>;
+  const int n = W.n, lane = W.lane;
+  // `cur` holds the batch of the position being staged, `nxt` the following one (loaded
+  // four positions ahead)
+  int4 cur = n > 0 ? __ldg(&W.row[0]) : make_int4(-1, -1, -1, -1);
+  int4 nxt = n > 4 ? __ldg(&W.row[1]) : make_int4(-1, -1, -1, -1);
+  int jc = n > 0 ? cur.x : -1;
+  // 2D records carry no type word: the neighbour's is read from the type array one
+  // position ahead, with its record's copy
+  int tc = DIM == 2 && jc >= 0 ? __ldg(&W.d.tinfo[jc]) : 0;
+  stage_records<Rec>(W.sb, W.rec, jc, lane);
+  cp_async_commit();
+  for (int k = 0; k < W.nmax; ++k) {
+    const int k1 = k + 1;
+    if ((k1 & 3) == 0) {
+      cur = nxt;
+      if (k1 + 4 < n) nxt = __ldg(&W.row[(k1 >> 2) + 1]);
+    }
+    const int q = k1 & 3;
+    const int jn = k1 < n ? (q == 0 ? cur.x : q == 1 ? cur.y : q == 2 ? cur.z : cur.w) : -1;
+    if (k1 < W.nmax) stage_records<Rec>(W.sb + (k1 & 1) * St::kRows, W.rec, jn, lane);
+    const int tn = DIM == 2 && jn >= 0 ? __ldg(&W.d.tinfo[jn]) : 0;
+    cp_async_commit();
+    cp_async_wait_prev();  // position k has landed (this lane's copies) ...
+    __syncwarp();          // ... and every other lane's
+    if (jc >= 0 && jc != W.i) {
+      const StagedRec<T, Rec> R(W.sb + (k & 1) * St::kRows + lane * St::kStride);
+      int tj;
+      if constexpr (DIM == 3) tj = type_of(R.r.tinfo); else tj = type_of(tc);
+      pair_term<T, DIM>(W.p, W.pp, W.cv, W.o, R.r, tj, acc);
+    }
+    __syncwarp();  // buffer k & 1 is refilled at position k + 2
+    jc = jn;
+    tc = tn;
+  }
+}
+
+// Two positions per step: the copies for positions k + 2, k + 3 are in flight while k and
+// k + 1 are evaluated, side by side where every lane's partners there are fluid.
+template <typename T, int DIM>
+__device__ __forceinline__ void pair_walk2(const PairWalk<T, DIM>& W, PairAcc<T, DIM>& acc) {
+  using Rec = typename RecFor<T, DIM>::type;
+  using St = PairStage<Rec>;
+  const int n = W.n, lane = W.lane;
+  int4 cur = n > 0 ? __ldg(&W.row[0]) : make_int4(-1, -1, -1, -1);
+  int4 nxt = n > 4 ? __ldg(&W.row[1]) : make_int4(-1, -1, -1, -1);
+  int ja = n > 0 ? cur.x : -1, jb = n > 1 ? cur.y : -1;
+  int ta = DIM == 2 && ja >= 0 ? __ldg(&W.d.tinfo[ja]) : 0;
+  int tb = DIM == 2 && jb >= 0 ? __ldg(&W.d.tinfo[jb]) : 0;
+  stage_records<Rec>(W.sb, W.rec, ja, lane);
+  stage_records<Rec>(W.sb + St::kRows, W.rec, jb, lane);
+  cp_async_commit();
+  for (int k = 0; k < W.nmax; k += 2) {
+    const int k2 = k + 2;
+    if ((k2 & 3) == 0) {
+      cur = nxt;
+      if (k2 + 4 < n) nxt = __ldg(&W.row[(k2 >> 2) + 1]);
+    }
+    const bool hi = (k2 & 2) != 0;
+    const int jna = k2 < n ? (hi ? cur.z : cur.x) : -1;
+    const int jnb = k2 + 1 < n ? (hi ? cur.w : cur.y) : -1;
+    if (k2 < W.nmax) {
+      int4* nbuf = W.sb + ((k2 >> 1) & 1) * 2 * St::kRows;
+      stage_records<Rec>(nbuf, W.rec, jna, lane);
+      stage_records<Rec>(nbuf + St::kRows, W.rec, jnb, lane);
+    }
+    const int tna = DIM == 2 && jna >= 0 ? __ldg(&W.d.tinfo[jna]) : 0;
+    const int tnb = DIM == 2 && jnb >= 0 ? __ldg(&W.d.tinfo[jnb]) : 0;
+    cp_async_commit();
+    cp_async_wait_prev();  // positions k, k + 1 have landed (this lane's copies) ...
+    __syncwarp();          // ... and every other lane's
+    const int4* src = W.sb + ((k >> 1) & 1) * 2 * St::kRows + lane * St::kStride;
+    const StagedRec<T, Rec> A(src), B(src + St::kRows);
+    const bool va = ja >= 0 && ja != W.i, vb = jb >= 0 && jb != W.i;
+    int tja, tjb;
+    if constexpr (DIM == 3) {
+      tja = type_of(A.r.tinfo);
+      tjb = type_of(B.r.tinfo);
+    } else {
+      tja = type_of(ta);
+      tjb = type_of(tb);
+    }
+    // side by side only where every lane of the warp qualifies: a warp split between the
+    // two forms would run both
+    if (__all_sync(SPH_FULL, W.o.fluid && (!va || tja == 0) && (!vb || tjb == 0))) {
+      pair_fluid_x2<T, DIM>(W.p, W.pp, W.o, A.r, va, B.r, vb, acc);
+    } else {
+      if (va) pair_term<T, DIM>(W.p, W.pp, W.cv, W.o, A.r, tja, acc);
+      if (vb) pair_term<T, DIM>(W.p, W.pp, W.cv, W.o, B.r, tjb, acc);
+    }
+    __syncwarp();  // this position pair's buffers are refilled at position k + 4
+    ja = jna;
+    jb = jnb;
+    ta = tna;
+    tb = tnb;
+  }
 }
 
 template <typename T, int DIM, int MODE, bool EXT>
-__global__ void __launch_bounds__(kPairWarps * 32, pair_min_blocks<T, DIM>()) k_pairs(Dev d) {
-  using Rec = typename RecFor<T, DIM>::type;
+__global__ void __launch_bounds__(PairShape<T, DIM>::kWarps * 32, PairShape<T, DIM>::kMinBlocks)
+    k_pairs(Dev d) {
+  using Sh = PairShape<T, DIM>;
+  using Rec = typename Sh::Rec;
   using St = PairStage<Rec>;
-  __shared__ int4 stage[kPairWarps][2][32 * St::kStride];
+  // per warp: a double buffer of kILP staged positions
+  __shared__ int4 stage[Sh::kWarps][2 * Sh::kILP][St::kRows];
   const int w = threadIdx.x >> 5, lane = threadIdx.x & 31;
-  const int wbase = (blockIdx.x * kPairWarps + w) * 32;
+  const int wbase = (blockIdx.x * Sh::kWarps + w) * 32;
   if (wbase >= d.Ntot) return;  // whole warps only: the lanes below cooperate
   const int i = wbase + lane;
   const bool active = i < d.Ntot;
@@ -962,54 +1110,12 @@ __global__ void __launch_bounds__(kPairWarps * 32, pair_min_blocks<T, DIM>()) k_
   int nmax = n;
 #pragma unroll
   for (int s = 16; s > 0; s >>= 1) nmax = max(nmax, __shfl_xor_sync(SPH_FULL, nmax, s));
-
-  // list row, read four indices at a time: `cur` holds the batch of the position being
-  // staged, `nxt` the following one (loaded four positions ahead)
-  const int4* __restrict__ row = reinterpret_cast<const int4*>(d.nbr + (size_t)is * d.cap);
-  int4 cur = n > 0 ? __ldg(&row[0]) : make_int4(-1, -1, -1, -1);
-  int4 nxt = n > 4 ? __ldg(&row[1]) : make_int4(-1, -1, -1, -1);
-  int4* sb = &stage[w][0][0];
-  int jc = n > 0 ? cur.x : -1;
-  // 2D records carry no type word: the neighbour's is read from the type array one
-  // position ahead, with its record's copy
-  int tc = DIM == 2 && jc >= 0 ? __ldg(&d.tinfo[jc]) : 0;
-  stage_records<Rec>(sb, rec, jc, lane);
-  cp_async_commit();
-  for (int k = 0; k < nmax; ++k) {
-    const int k1 = k + 1;
-    if ((k1 & 3) == 0) {
-      cur = nxt;
-      if (k1 + 4 < n) nxt = __ldg(&row[(k1 >> 2) + 1]);
-    }
-    const int q = k1 & 3;
-    const int jn = k1 < n ? (q == 0 ? cur.x : q == 1 ? cur.y : q == 2 ? cur.z : cur.w) : -1;
-    if (k1 < nmax) stage_records<Rec>(sb + (k1 & 1) * 32 * St::kStride, rec, jn, lane);
-    const int tn = DIM == 2 && jn >= 0 ? __ldg(&d.tinfo[jn]) : 0;
-    cp_async_commit();
-    cp_async_wait_prev();  // position k has landed (this lane's copies) ...
-    __syncwarp();          // ... and every other lane's
-    if (jc >= 0 && jc != i) {
-      const int4* src = sb + (k & 1) * 32 * St::kStride + lane * St::kStride;
-      if constexpr (sizeof(T) == 8) {
-        // FP64: the neighbour's record is read in place, each field loaded where the pair
-        // term uses it, which keeps the 128-byte record out of the register file
-        const Rec& rj = *reinterpret_cast<const Rec*>(src);
-        int tj;
-        if constexpr (DIM == 3) tj = type_of(rj.tinfo); else tj = type_of(tc);
-        pair_term<T, DIM>(p, pp, cv, o, rj, tj, acc);
-      } else {
-        typename St::Slot rj;
-#pragma unroll
-        for (int t = 0; t < St::kPieces; ++t) rj.v[t] = src[t];
-        int tj;
-        if constexpr (DIM == 3) tj = type_of(rj.r.tinfo); else tj = type_of(tc);
-        pair_term<T, DIM>(p, pp, cv, o, rj.r, tj, acc);
-      }
-    }
-    __syncwarp();  // buffer k & 1 is refilled at position k + 2
-    jc = jn;
-    tc = tn;
-  }
+  const PairWalk<T, DIM> W{d, rec, reinterpret_cast<const int4*>(d.nbr + (size_t)is * d.cap),
+                           &stage[w][0][0], lane, i, n, nmax, p, pp, cv, o};
+  if constexpr (Sh::kILP == 2)
+    pair_walk2<T, DIM>(W, acc);
+  else
+    pair_walk1<T, DIM>(W, acc);
   if (active) pair_store<T, DIM, MODE, EXT>(d, i, p, o, acc);
 }
 
@@ -1599,8 +1705,9 @@ int launch_pressure(const Launch& L) {
 }
 
 template <typename T, int DIM>
-static void pairs_dispatch(const Launch& L, int mode, int with_ext, int nb) {
-  constexpr int nt = kPairWarps * 32;
+static void pairs_dispatch(const Launch& L, int mode, int with_ext) {
+  constexpr int nt = PairShape<T, DIM>::kWarps * 32;
+  const int nb = blocks(L.d.Ntot, nt);
   if (mode == kPairGradvAll)
     k_pairs<T, DIM, kPairGradvAll, false><<<nb, nt, 0, S(L)>>>(L.d);
   else if (mode == kPairForcesOnly)
@@ -1613,13 +1720,12 @@ static void pairs_dispatch(const Launch& L, int mode, int with_ext, int nb) {
 
 int launch_pairs_dim(const Launch& L, int dim, int mode, int with_ext) {
   if (L.d.Ntot == 0) return 0;
-  const int nb = blocks(L.d.Ntot, kPairWarps * 32);
   if (L.prec == SPH_PREC_FP64) {
-    if (dim == 3) pairs_dispatch<double, 3>(L, mode, with_ext, nb);
-    else pairs_dispatch<double, 2>(L, mode, with_ext, nb);
+    if (dim == 3) pairs_dispatch<double, 3>(L, mode, with_ext);
+    else pairs_dispatch<double, 2>(L, mode, with_ext);
   } else {
-    if (dim == 3) pairs_dispatch<float, 3>(L, mode, with_ext, nb);
-    else pairs_dispatch<float, 2>(L, mode, with_ext, nb);
+    if (dim == 3) pairs_dispatch<float, 3>(L, mode, with_ext);
+    else pairs_dispatch<float, 2>(L, mode, with_ext);
   }
   return check(L);
 }
