@@ -50,6 +50,7 @@ enum Epi { kEpiStore = 0, kEpiForward = 1, kEpiBackward = 2 };
 struct EpiArgs {
   float* C;                 // kEpiStore: FP32 result, ldc = N
   long long strideC;
+  long long strideSplit;    // kEpiStore with split K: distance between the slices' results
   const float* bias;        // kEpiForward: + bias[col], then GELU
   long long strideBias;
   const float* Zin;         // kEpiBackward: GELU'(Zin) of the layer below
@@ -81,7 +82,7 @@ __global__ void __launch_bounds__(128, 1) k_gemm(GemmArgs g, EpiArgs e) {
       float v[16];
       tc::tmem_ld16(tmem + ((uint32_t)(warp * 32) << 16) + (uint32_t)c0, v);
       if (EPI == kEpiStore) {
-        float* c = e.C + head * e.strideC + (size_t)row * N + c0;
+        float* c = e.C + blockIdx.z * e.strideSplit + head * e.strideC + (size_t)row * N + c0;
 #pragma unroll
         for (int q = 0; q < 16; q += 4)
           *reinterpret_cast<float4*>(c + q) = make_float4(v[q], v[q + 1], v[q + 2], v[q + 3]);
@@ -118,6 +119,17 @@ __global__ void __launch_bounds__(128, 1) k_gemm(GemmArgs g, EpiArgs e) {
     tc::fence_after_sync();
     tc::tmem_free(tmem, tc::kTmemCols);
   }
+}
+
+// Sum of the split-K slices of a weight gradient in slice order (a fixed order: training
+// stays bit-reproducible): C[h * strideC + i] = sum over s of ws[(s * heads + h) * MN + i].
+__global__ void k_sum_splits(const float* __restrict__ ws, int splits, int heads, int MN,
+                             float* __restrict__ C, long long strideC) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x, h = blockIdx.y;
+  if (i >= MN) return;
+  float acc = ws[(size_t)h * MN + i];
+  for (int s = 1; s < splits; ++s) acc += ws[((size_t)s * heads + h) * MN + i];
+  C[h * strideC + i] = acc;
 }
 
 // ---- CUDA-core layers (6-wide input, 4-wide output) ----
@@ -343,6 +355,7 @@ struct sph_mlp {
                 *h3t = nullptr, *dz1 = nullptr, *dz1t = nullptr, *dz2 = nullptr, *dz2t = nullptr,
                 *dz3 = nullptr, *dz3t = nullptr;
   float *out = nullptr, *dout = nullptr, *sqerr = nullptr, *loss = nullptr;
+  float* ws = nullptr;  // split-K slices of a weight gradient (kMaxSplits x heads x HID x HID)
   int* err = nullptr;
   long long step = 0;
 };
@@ -394,7 +407,7 @@ void init_params(std::vector<float>& P, int heads, unsigned long long seed) {
 
 template <int EPI>
 int gemm_launch(sph_mlp* c, const __nv_bfloat16* A, long long sA, int lda, const __nv_bfloat16* B,
-                long long sB, int ldb, int M, int N, int K, const EpiArgs& e) {
+                long long sB, int ldb, int M, int N, int K, const EpiArgs& e, int splits = 1) {
   GemmArgs g;
   g.A = A;
   g.B = B;
@@ -406,7 +419,31 @@ int gemm_launch(sph_mlp* c, const __nv_bfloat16* A, long long sA, int lda, const
   g.N = N;
   g.K = K;
   g.err = c->err;
-  k_gemm<EPI><<<dim3(M / tc::kTileM, c->heads), 128, tc::kSmemBytes, c->stream>>>(g, e);
+  k_gemm<EPI><<<dim3(M / tc::kTileM, c->heads, splits), 128, tc::kSmemBytes, c->stream>>>(g, e);
+  return cudaGetLastError() != cudaSuccess;
+}
+
+// Weight gradient dW = dZ^T H (M = N = HID, K = the batch) into grads + off of every head.
+// The K = batch reduction is split over up to kMaxSplits CTAs per output tile (2 tiles per
+// head leave most SMs idle otherwise); the slices are summed in order by k_sum_splits.
+constexpr int kMaxSplits = 8;
+int weight_grad(sph_mlp* c, const __nv_bfloat16* dzt, const __nv_bfloat16* ht, int B, int off) {
+  const long long act = (long long)B * HID;
+  int splits = kMaxSplits;
+  while (splits > 1 && B % (tc::kChunkK * splits) != 0) splits /= 2;
+  EpiArgs e{};
+  if (splits == 1) {
+    e.C = c->grads + off;
+    e.strideC = NPARAM;
+    return gemm_launch<kEpiStore>(c, dzt, act, B, ht, act, B, HID, HID, B, e);
+  }
+  const int MN = HID * HID;
+  e.C = c->ws;
+  e.strideC = MN;
+  e.strideSplit = (long long)c->heads * MN;
+  if (gemm_launch<kEpiStore>(c, dzt, act, B, ht, act, B, HID, HID, B, e, splits)) return 1;
+  k_sum_splits<<<dim3((MN + 255) / 256, c->heads), 256, 0, c->stream>>>(c->ws, splits, c->heads,
+                                                                          MN, c->grads + off, NPARAM);
   return cudaGetLastError() != cudaSuccess;
 }
 
@@ -451,8 +488,7 @@ int backward(sph_mlp* c, const float* x, int B) {
   e.strideZ = act;
   e.strideH = act;
   // dW3 = dz3^T h2, then dz2 = (dz3 W3) * GELU'(z2)
-  e.C = c->grads + OFF_W3;
-  if (gemm_launch<kEpiStore>(c, c->dz3t, act, B, c->h2t, act, B, HID, HID, B, e)) return 1;
+  if (weight_grad(c, c->dz3t, c->h2t, B, OFF_W3)) return 1;
   e.Zin = c->z2;
   e.H = c->dz2;
   e.Ht = c->dz2t;
@@ -460,8 +496,7 @@ int backward(sph_mlp* c, const float* x, int B) {
                                 HID, e))
     return 1;
   // dW2 = dz2^T h1, then dz1 = (dz2 W2) * GELU'(z1)
-  e.C = c->grads + OFF_W2;
-  if (gemm_launch<kEpiStore>(c, c->dz2t, act, B, c->h1t, act, B, HID, HID, B, e)) return 1;
+  if (weight_grad(c, c->dz2t, c->h1t, B, OFF_W2)) return 1;
   e.Zin = c->z1;
   e.H = c->dz1;
   e.Ht = c->dz1t;
@@ -563,7 +598,7 @@ sph_status sph_mlp_create(int heads, int max_batch, unsigned long long seed, int
   ok = ok && mlp_alloc(c, &c->out, (size_t)heads * max_batch * OUT) &&
        mlp_alloc(c, &c->dout, (size_t)heads * max_batch * OUT) &&
        mlp_alloc(c, &c->sqerr, (size_t)heads * max_batch) && mlp_alloc(c, &c->loss, heads) &&
-       mlp_alloc(c, &c->err, 1);
+       mlp_alloc(c, &c->ws, (size_t)kMaxSplits * heads * HID * HID) && mlp_alloc(c, &c->err, 1);
   if (!ok) {
     mlp_free(c);
     return SPH_ERR_NOMEM;

@@ -149,11 +149,15 @@ __device__ __forceinline__ void load_chunk(uint8_t* dst, const __nv_bfloat16* sr
 }
 
 // The main loop: leaves the 128 x N FP32 accumulator of this CTA's tile in TMEM columns
-// [tmem, tmem + N).  Returns false if an MMA completion was not observed in time.
+// [tmem, tmem + N).  With gridDim.z > 1 the CTA takes K slice blockIdx.z of gridDim.z equal
+// slices (split K; K / gridDim.z a multiple of 64).  Returns false if an MMA completion was
+// not observed in time.
 __device__ __forceinline__ bool gemm_mainloop(const GemmArgs& g, uint8_t* smem, uint64_t* bar,
                                               uint32_t tmem) {
   const int head = blockIdx.y;
   const int m0 = blockIdx.x * kTileM;
+  const int kslice = g.K / (int)gridDim.z;
+  const int kb = (int)blockIdx.z * kslice, ke = kb + kslice;
   const __nv_bfloat16* A = g.A + head * g.strideA;
   const __nv_bfloat16* B = g.B + head * g.strideB;
   uint8_t* sA = smem;
@@ -161,7 +165,7 @@ __device__ __forceinline__ bool gemm_mainloop(const GemmArgs& g, uint8_t* smem, 
   const uint32_t idesc = idesc_bf16_f32(kTileM, g.N);
   uint32_t parity = 0;
   bool ok = true;
-  for (int k0 = 0; k0 < g.K; k0 += kChunkK) {
+  for (int k0 = kb; k0 < ke; k0 += kChunkK) {
     load_chunk(sA, A, g.lda, m0, kTileM, k0);
     load_chunk(sB, B, g.ldb, 0, g.N, k0);
     // generic-proxy stores -> visible to the tensor core's (async proxy) reads
@@ -173,7 +177,7 @@ __device__ __forceinline__ bool gemm_mainloop(const GemmArgs& g, uint8_t* smem, 
 #pragma unroll
       for (int s = 0; s < kChunkK / 16; ++s)
         mma_bf16(tmem, smem_desc(smem_u32(sA) + s * 256), smem_desc(smem_u32(sB) + s * 256),
-                 idesc, (k0 > 0 || s > 0) ? 1 : 0);
+                 idesc, (k0 > kb || s > 0) ? 1 : 0);
       mma_commit(bar);
     }
     // the next chunk overwrites sA / sB: wait until the MMAs have consumed them
