@@ -138,14 +138,20 @@ struct GemmArgs {
 };
 
 // Copies rows [r0, r0 + rows) x K-chunk [k0, k0 + 64) of a K-contiguous bf16 matrix into
-// the canonical layout at dst.
+// the canonical layout at dst: 16-byte cp.async copies, all of the thread's in flight at
+// once (completed by cp_async_wait_all).
 __device__ __forceinline__ void load_chunk(uint8_t* dst, const __nv_bfloat16* src, int ld, int r0,
                                            int rows, int k0) {
   for (int idx = threadIdx.x; idx < rows * (kChunkK / 8); idx += blockDim.x) {
     const int r = idx >> 3, k8 = idx & 7;
-    const uint4 v = *reinterpret_cast<const uint4*>(src + (size_t)(r0 + r) * ld + k0 + k8 * 8);
-    *reinterpret_cast<uint4*>(dst + core_offset(r, k8)) = v;
+    asm volatile("cp.async.cg.shared.global [%0], [%1], 16;\n" ::"r"(
+                     smem_u32(dst + core_offset(r, k8))),
+                 "l"(src + (size_t)(r0 + r) * ld + k0 + k8 * 8)
+                 : "memory");
   }
+}
+__device__ __forceinline__ void cp_async_wait_all() {
+  asm volatile("cp.async.commit_group;\ncp.async.wait_group 0;\n" ::: "memory");
 }
 
 // The main loop: leaves the 128 x N FP32 accumulator of this CTA's tile in TMEM columns
@@ -168,6 +174,7 @@ __device__ __forceinline__ bool gemm_mainloop(const GemmArgs& g, uint8_t* smem, 
   for (int k0 = kb; k0 < ke; k0 += kChunkK) {
     load_chunk(sA, A, g.lda, m0, kTileM, k0);
     load_chunk(sB, B, g.ldb, 0, g.N, k0);
+    cp_async_wait_all();
     // generic-proxy stores -> visible to the tensor core's (async proxy) reads
     asm volatile("fence.proxy.async.shared::cta;\n" ::: "memory");
     fence_before_sync();
