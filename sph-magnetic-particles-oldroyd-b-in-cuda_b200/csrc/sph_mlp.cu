@@ -64,16 +64,19 @@ struct EpiArgs {
 template <int EPI>
 __global__ void __launch_bounds__(128, 1) k_gemm(GemmArgs g, EpiArgs e) {
   extern __shared__ __align__(1024) uint8_t smem[];
-  __shared__ uint64_t bar;
+  __shared__ uint64_t bar[2];
   __shared__ uint32_t tmem_sh;
   const int warp = threadIdx.x >> 5;
   if (warp == 0) tc::tmem_alloc(&tmem_sh, tc::kTmemCols);
-  if (threadIdx.x == 0) tc::mbar_init(&bar, 1);
+  if (threadIdx.x == 0) {
+    tc::mbar_init(&bar[0], 1);
+    tc::mbar_init(&bar[1], 1);
+  }
   tc::fence_before_sync();
   __syncthreads();
   tc::fence_after_sync();
   const uint32_t tmem = tmem_sh;
-  const bool ok = __syncthreads_and(tc::gemm_mainloop(g, smem, &bar, tmem));
+  const bool ok = __syncthreads_and(tc::gemm_mainloop(g, smem, bar, tmem));
   if (ok) {
     const int head = blockIdx.y;
     const int row = blockIdx.x * tc::kTileM + threadIdx.x;
@@ -306,16 +309,19 @@ __global__ void k_loss(const float* sqerr, int B, float* loss) {
 __global__ void __launch_bounds__(128, 1) k_gemm_f32(GemmArgs g, float* C, int ldc,
                                                       long long strideC) {
   extern __shared__ __align__(1024) uint8_t smem[];
-  __shared__ uint64_t bar;
+  __shared__ uint64_t bar[2];
   __shared__ uint32_t tmem_sh;
   const int warp = threadIdx.x >> 5;
   if (warp == 0) tc::tmem_alloc(&tmem_sh, tc::kTmemCols);
-  if (threadIdx.x == 0) tc::mbar_init(&bar, 1);
+  if (threadIdx.x == 0) {
+    tc::mbar_init(&bar[0], 1);
+    tc::mbar_init(&bar[1], 1);
+  }
   tc::fence_before_sync();
   __syncthreads();
   tc::fence_after_sync();
   const uint32_t tmem = tmem_sh;
-  const bool ok = __syncthreads_and(tc::gemm_mainloop(g, smem, &bar, tmem));
+  const bool ok = __syncthreads_and(tc::gemm_mainloop(g, smem, bar, tmem));
   if (ok) {
     const int row = blockIdx.x * tc::kTileM + threadIdx.x;
     float* c = C + blockIdx.y * strideC + (size_t)row * ldc;

@@ -156,42 +156,61 @@ __device__ __forceinline__ void cp_async_wait_all() {
 
 // The main loop: leaves the 128 x N FP32 accumulator of this CTA's tile in TMEM columns
 // [tmem, tmem + N).  With gridDim.z > 1 the CTA takes K slice blockIdx.z of gridDim.z equal
-// slices (split K; K / gridDim.z a multiple of 64).  Returns false if an MMA completion was
-// not observed in time.
+// slices (split K; K / gridDim.z a multiple of 64).  Two stages: the copies of chunk c + 1
+// are in flight while the MMAs of chunk c run; bar[s] counts the MMA completions of stage s
+// (a stage is refilled only after the MMAs that read it are done).  Returns false if an
+// MMA completion was not observed in time.
+constexpr int kStageA = kTileM * kChunkK * 2;
+constexpr int kStageBytes = kStageA + kMaxN * kChunkK * 2;
+static_assert(2 * kStageBytes <= kSmemBytes, "two stages of A and B chunks");
 __device__ __forceinline__ bool gemm_mainloop(const GemmArgs& g, uint8_t* smem, uint64_t* bar,
                                               uint32_t tmem) {
   const int head = blockIdx.y;
   const int m0 = blockIdx.x * kTileM;
   const int kslice = g.K / (int)gridDim.z;
-  const int kb = (int)blockIdx.z * kslice, ke = kb + kslice;
+  const int kb = (int)blockIdx.z * kslice;
+  const int nch = kslice / kChunkK;
   const __nv_bfloat16* A = g.A + head * g.strideA;
   const __nv_bfloat16* B = g.B + head * g.strideB;
-  uint8_t* sA = smem;
-  uint8_t* sB = smem + kTileM * kChunkK * 2;
   const uint32_t idesc = idesc_bf16_f32(kTileM, g.N);
-  uint32_t parity = 0;
-  bool ok = true;
-  for (int k0 = kb; k0 < ke; k0 += kChunkK) {
-    load_chunk(sA, A, g.lda, m0, kTileM, k0);
-    load_chunk(sB, B, g.ldb, 0, g.N, k0);
+  auto fill = [&](int c) {
+    uint8_t* st = smem + (c & 1) * kStageBytes;
+    load_chunk(st, A, g.lda, m0, kTileM, kb + c * kChunkK);
+    load_chunk(st + kStageA, B, g.ldb, 0, g.N, kb + c * kChunkK);
     cp_async_wait_all();
     // generic-proxy stores -> visible to the tensor core's (async proxy) reads
     asm volatile("fence.proxy.async.shared::cta;\n" ::: "memory");
     fence_before_sync();
     __syncthreads();
     fence_after_sync();
+  };
+  bool ok = true;
+  if (nch > 0) fill(0);
+  for (int c = 0; c < nch; ++c) {
+    const int s = c & 1;
     if (threadIdx.x == 0) {
+      const uint32_t sa = smem_u32(smem + s * kStageBytes), sb = sa + kStageA;
 #pragma unroll
-      for (int s = 0; s < kChunkK / 16; ++s)
-        mma_bf16(tmem, smem_desc(smem_u32(sA) + s * 256), smem_desc(smem_u32(sB) + s * 256),
-                 idesc, (k0 > kb || s > 0) ? 1 : 0);
-      mma_commit(bar);
+      for (int q = 0; q < kChunkK / 16; ++q)
+        mma_bf16(tmem, smem_desc(sa + q * 256), smem_desc(sb + q * 256), idesc,
+                 (c > 0 || q > 0) ? 1 : 0);
+      mma_commit(&bar[s]);
     }
-    // the next chunk overwrites sA / sB: wait until the MMAs have consumed them
-    ok = mbar_wait(bar, parity) && ok;
-    parity ^= 1u;
+    if (c + 1 < nch) {
+      // stage s ^ 1 was read by the MMAs of chunk c - 1 (commit number (c - 1) / 2 of its
+      // barrier); every earlier commit of that barrier has been waited for
+      if (c >= 1) {
+        ok = mbar_wait(&bar[s ^ 1], (uint32_t)(((c - 1) >> 1) & 1)) && ok;
+        fence_after_sync();
+      }
+      if (!ok) break;
+      fill(c + 1);
+    }
+  }
+  // the last commit completes after every MMA before it
+  if (ok && nch > 0) {
+    ok = mbar_wait(&bar[(nch - 1) & 1], (uint32_t)(((nch - 1) >> 1) & 1));
     fence_after_sync();
-    if (!ok) break;
   }
   return ok;
 }
