@@ -79,11 +79,12 @@ __global__ void __launch_bounds__(128, 1) k_gemm(GemmArgs g, EpiArgs e) {
   const bool ok = __syncthreads_and(tc::gemm_mainloop(g, smem, bar, tmem));
   if (ok) {
     const int head = blockIdx.y;
-    const int row = blockIdx.x * tc::kTileM + threadIdx.x;
+    const int row = tc::tile_m0(g) + threadIdx.x, n0 = tc::tile_n0(g);
     const int N = g.N, M = g.M;
-    for (int c0 = 0; c0 < N; c0 += 16) {
+    for (int t0 = 0; t0 < g.ntile; t0 += 16) {
       float v[16];
-      tc::tmem_ld16(tmem + ((uint32_t)(warp * 32) << 16) + (uint32_t)c0, v);
+      tc::tmem_ld16(tmem + ((uint32_t)(warp * 32) << 16) + (uint32_t)t0, v);
+      const int c0 = n0 + t0;  // output column
       if (EPI == kEpiStore) {
         float* c = e.C + blockIdx.z * e.strideSplit + head * e.strideC + (size_t)row * N + c0;
 #pragma unroll
@@ -323,9 +324,9 @@ __global__ void __launch_bounds__(128, 1) k_gemm_f32(GemmArgs g, float* C, int l
   const uint32_t tmem = tmem_sh;
   const bool ok = __syncthreads_and(tc::gemm_mainloop(g, smem, bar, tmem));
   if (ok) {
-    const int row = blockIdx.x * tc::kTileM + threadIdx.x;
-    float* c = C + blockIdx.y * strideC + (size_t)row * ldc;
-    for (int c0 = 0; c0 < g.N; c0 += 16) {
+    const int row = tc::tile_m0(g) + threadIdx.x;
+    float* c = C + blockIdx.y * strideC + (size_t)row * ldc + tc::tile_n0(g);
+    for (int c0 = 0; c0 < g.ntile; c0 += 16) {
       float v[16];
       tc::tmem_ld16(tmem + ((uint32_t)(warp * 32) << 16) + (uint32_t)c0, v);
 #pragma unroll
@@ -424,8 +425,12 @@ int gemm_launch(sph_mlp* c, const __nv_bfloat16* A, long long sA, int lda, const
   g.M = M;
   g.N = N;
   g.K = K;
+  // the 1024-row forward and input-gradient GEMMs: two column tiles per row tile (80 CTAs
+  // for 5 heads instead of 40)
+  g.ntile = (EPI != kEpiStore && N == 256 && M >= 512) ? 128 : N;
   g.err = c->err;
-  k_gemm<EPI><<<dim3(M / tc::kTileM, c->heads, splits), 128, tc::kSmemBytes, c->stream>>>(g, e);
+  k_gemm<EPI><<<dim3(M / tc::kTileM * (N / g.ntile), c->heads, splits), 128, tc::kSmemBytes,
+                 c->stream>>>(g, e);
   return cudaGetLastError() != cudaSuccess;
 }
 
@@ -561,6 +566,7 @@ sph_status sph_tc_gemm(const void* A, const void* B, float* C, int M, int N, int
   g.M = M;
   g.N = N;
   g.K = K;
+  g.ntile = N;
   g.err = err;
   k_gemm_f32<<<dim3(M / tc::kTileM, heads), 128, tc::kSmemBytes, st>>>(g, C, N, (long long)M * N);
   int h = 0;

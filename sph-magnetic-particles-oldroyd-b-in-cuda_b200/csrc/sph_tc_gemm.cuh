@@ -134,8 +134,17 @@ struct GemmArgs {
   long long strideA, strideB;
   int lda, ldb;  // row pitch (elements), multiples of 8
   int M, N, K;   // M % 128 == 0, N % 16 == 0 and N <= 256, K % 64 == 0
+  int ntile;     // columns per CTA (N, or a divisor of N that is a multiple of 16)
   int* err;      // set to 1 when a wait gives up
 };
+
+// The CTA's output tile: blockIdx.x enumerates (row tile, column tile), column tile fastest.
+__device__ __forceinline__ int tile_m0(const GemmArgs& g) {
+  return (int)(blockIdx.x / (g.N / g.ntile)) * kTileM;
+}
+__device__ __forceinline__ int tile_n0(const GemmArgs& g) {
+  return (int)(blockIdx.x % (g.N / g.ntile)) * g.ntile;
+}
 
 // Copies rows [r0, r0 + rows) x K-chunk [k0, k0 + 64) of a K-contiguous bf16 matrix into
 // the canonical layout at dst: 16-byte cp.async copies, all of the thread's in flight at
@@ -154,8 +163,8 @@ __device__ __forceinline__ void cp_async_wait_all() {
   asm volatile("cp.async.commit_group;\ncp.async.wait_group 0;\n" ::: "memory");
 }
 
-// The main loop: leaves the 128 x N FP32 accumulator of this CTA's tile in TMEM columns
-// [tmem, tmem + N).  With gridDim.z > 1 the CTA takes K slice blockIdx.z of gridDim.z equal
+// The main loop: leaves the 128 x ntile FP32 accumulator of this CTA's tile in TMEM columns
+// [tmem, tmem + ntile).  With gridDim.z > 1 the CTA takes K slice blockIdx.z of gridDim.z equal
 // slices (split K; K / gridDim.z a multiple of 64).  Two stages: the copies of chunk c + 1
 // are in flight while the MMAs of chunk c run; bar[s] counts the MMA completions of stage s
 // (a stage is refilled only after the MMAs that read it are done).  Returns false if an
@@ -166,17 +175,17 @@ static_assert(2 * kStageBytes <= kSmemBytes, "two stages of A and B chunks");
 __device__ __forceinline__ bool gemm_mainloop(const GemmArgs& g, uint8_t* smem, uint64_t* bar,
                                               uint32_t tmem) {
   const int head = blockIdx.y;
-  const int m0 = blockIdx.x * kTileM;
+  const int m0 = tile_m0(g), n0 = tile_n0(g);
   const int kslice = g.K / (int)gridDim.z;
   const int kb = (int)blockIdx.z * kslice;
   const int nch = kslice / kChunkK;
   const __nv_bfloat16* A = g.A + head * g.strideA;
   const __nv_bfloat16* B = g.B + head * g.strideB;
-  const uint32_t idesc = idesc_bf16_f32(kTileM, g.N);
+  const uint32_t idesc = idesc_bf16_f32(kTileM, g.ntile);
   auto fill = [&](int c) {
     uint8_t* st = smem + (c & 1) * kStageBytes;
     load_chunk(st, A, g.lda, m0, kTileM, kb + c * kChunkK);
-    load_chunk(st + kStageA, B, g.ldb, 0, g.N, kb + c * kChunkK);
+    load_chunk(st + kStageA, B, g.ldb, n0, g.ntile, kb + c * kChunkK);
     cp_async_wait_all();
     // generic-proxy stores -> visible to the tensor core's (async proxy) reads
     asm volatile("fence.proxy.async.shared::cta;\n" ::: "memory");
