@@ -322,9 +322,7 @@ __device__ __forceinline__ void density_epilogue(const Dev& d, int i, const BoxP
 // its lanes idle.  The lists are the same either way (same candidates, same order).
 //
 // Blocks of 4 warps, measured against 8 (128^3 list build 1.66 vs 1.88 ms; 2D ensemble
-// 1.15 vs 1.19 ms with the test loop not unrolled).  A block then holds half the shared
-// memory, and more of the SM's on-chip storage is left to L1, where the candidate
-// positions that 27 neighbouring cells load in turn are reused.
+// 1.15 vs 1.19 ms, with the test loop not unrolled).
 constexpr int kListWarps = 4;
 
 // Packed FP32 pairs (the f32x2 arithmetic of sm_100): two candidates per instruction.
