@@ -49,12 +49,15 @@ def _batch(n, seed):
     return x, y
 
 
-def test_mlp_gradients_match_fp64_oracle():
+@pytest.mark.parametrize("batch", [256, 1024])
+def test_mlp_gradients_match_fp64_oracle(batch):
+    """Batch 256: the weight gradients split K over 4 CTAs per tile; batch 1024: over 8, and
+    the forward and input-gradient GEMMs take two column tiles per row tile."""
     import mlp_oracle
     import sph_surrogate
 
-    net = sph_surrogate.MLP(heads=2, max_batch=256, seed=3)
-    x, y = _batch(256, 1)
+    net = sph_surrogate.MLP(heads=2, max_batch=batch, seed=3)
+    x, y = _batch(batch, 1)
     loss, g = net.gradients(x, y)
     P = net.get_params()
     xs, ys = x.cpu().numpy(), y.cpu().numpy()
