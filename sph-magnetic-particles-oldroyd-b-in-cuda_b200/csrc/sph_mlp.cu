@@ -352,6 +352,7 @@ bool gemm_shape_ok(int M, int N, int K) {
 
 struct sph_mlp {
   int heads = 0, max_batch = 0, device = 0;
+  int nsm = 148;  // multiprocessors of the device
   cudaStream_t stream = nullptr;  // cudaStreamLegacy
   std::vector<void*> allocs;
   float *params = nullptr, *grads = nullptr, *m = nullptr, *v = nullptr;
@@ -425,9 +426,9 @@ int gemm_launch(sph_mlp* c, const __nv_bfloat16* A, long long sA, int lda, const
   g.M = M;
   g.N = N;
   g.K = K;
-  // the 1024-row forward and input-gradient GEMMs: two column tiles per row tile (80 CTAs
-  // for 5 heads instead of 40)
-  g.ntile = (EPI != kEpiStore && N == 256 && M >= 512) ? 128 : N;
+  // forward and input-gradient GEMMs whose row tiles alone leave SMs idle (a 1024-sample
+  // batch: 8 row tiles x 5 heads = 40 CTAs): two column tiles per row tile
+  g.ntile = (EPI != kEpiStore && N == 256 && (M / tc::kTileM) * c->heads < c->nsm) ? 128 : N;
   g.err = c->err;
   k_gemm<EPI><<<dim3(M / tc::kTileM * (N / g.ntile), c->heads, splits), 128, tc::kSmemBytes,
                  c->stream>>>(g, e);
@@ -592,6 +593,7 @@ sph_status sph_mlp_create(int heads, int max_batch, unsigned long long seed, int
   c->heads = heads;
   c->max_batch = max_batch;
   c->device = device;
+  cudaDeviceGetAttribute(&c->nsm, cudaDevAttrMultiProcessorCount, device);
   // the legacy default stream: the caller's inputs (batches made by default-stream work,
   // e.g. a framework's allocator) are then ordered before, and their reuse after, the
   // network's kernels
