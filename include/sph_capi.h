@@ -303,9 +303,12 @@ sph_status sph_kernel_launches(const sph_ctx* ctx, long long* count);
    occupied cells only and keep earlier values elsewhere, as the reference's arrays do.
    The sort's scratch is a static device array of the library sized for at most
    SPH_NOALLOC_MAX_PARTICLES particles (about 13 MB, held by every GPU that loads the
-   library until the process exits); larger n returns SPH_ERR_CAPACITY.  The first call
-   on a device looks up that array's device address (once per device).  All calls share
-   the array: calls that overlap on the GPU race, so serialise them.  The call runs on
+   library until the process exits); larger n returns SPH_ERR_CAPACITY.  Every call looks
+   up that array's device address in the current context (cheap; nothing is cached, so a
+   call after cudaDeviceReset finds the array's new address).  The first call in a context
+   loads the library's device code for this entry point, which places the array; make
+   that first call (n = 0 is enough) before any stream capture.  All calls share the
+   array: calls that overlap on the GPU race, so serialise them.  The call runs on
    `stream` (a cudaStream_t, NULL for the default stream) and waits for it before it
    returns; a particle outside the grid gives SPH_ERR_CELL_RANGE. */
 #define SPH_NOALLOC_MAX_PARTICLES (1 << 20)

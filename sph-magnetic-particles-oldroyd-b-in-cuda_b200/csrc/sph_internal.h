@@ -272,6 +272,19 @@ int launch_init_scatter(const Launch& L, int n, const int2* meta, const double4*
 
 // Stable LSD radix sort of the hash keys (sph_sort.cu): keys d.key_by_gid indexed by
 // global id, values = global ids; result in d.keys / d.vals.
+// Geometry of the sort, shared by every user of its histogram buffer: items per tile,
+// buckets per pass (at most 9 key bits per pass) and entries per scan block.
+constexpr int kSortTile = 4096;
+constexpr int kSortMaxBuckets = 512;
+constexpr int kSortScanChunk = 2048;
+// Histogram ints the sort needs for n keys: a bucket-major table of kSortMaxBuckets
+// counters per tile, one partial sum per scan block, and padding.
+constexpr size_t sort_hist_ints(long long n) {
+  return (size_t)kSortMaxBuckets * (size_t)(n > 0 ? (n + kSortTile - 1) / kSortTile : 1) +
+         ((size_t)kSortMaxBuckets * (size_t)(n > 0 ? (n + kSortTile - 1) / kSortTile : 1) +
+          kSortScanChunk - 1) / kSortScanChunk +
+         32;
+}
 struct SortScratch {
   int* hist;       // radix histogram / offsets
   int hist_len;
@@ -279,7 +292,5 @@ struct SortScratch {
 };
 size_t sort_hist_len(int n, int key_bits);
 int launch_sort(const Launch& L, int key_bits, const SortScratch& scr);
-
-size_t sort_hist_len(int n, int key_bits);
 
 }  // namespace sph

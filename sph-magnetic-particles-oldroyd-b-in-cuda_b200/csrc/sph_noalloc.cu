@@ -16,7 +16,6 @@
 #include <cuda_runtime.h>
 
 #include <cmath>
-#include <mutex>
 
 #include "sph_internal.h"
 
@@ -29,8 +28,8 @@ int launch_sort_buffers(const int* keys_in, int n, int key_bits, int* keys_out, 
 namespace {
 
 constexpr int kMaxN = SPH_NOALLOC_MAX_PARTICLES;
-constexpr int kSortTile = 4096;                                   // sph_sort.cu kTile
-constexpr int kHistInts = 512 * ((kMaxN + kSortTile - 1) / kSortTile) + 1024;
+// the sort's histogram for kMaxN keys, sized by the sort's own geometry (sph_internal.h)
+constexpr size_t kHistInts = sph::sort_hist_ints(kMaxN);
 // layout (ints): unsorted keys | ping-pong keys | ping-pong values | histogram | status
 constexpr size_t kOffKeys = 0;
 constexpr size_t kOffTmpK = kOffKeys + kMaxN;
@@ -40,10 +39,6 @@ constexpr size_t kOffStatus = kOffHist + kHistInts;
 constexpr size_t kScratchInts = kOffStatus + 64;
 
 __device__ __align__(256) int g_noalloc_scratch[kScratchInts];
-
-// Device address of g_noalloc_scratch per device; host code may not use the symbol itself.
-std::mutex g_setup_mutex;
-int* g_scratch_ptr[256] = {nullptr};
 
 __global__ void k_noalloc_hash(const double* __restrict__ x, const double* __restrict__ y,
                                const double* __restrict__ z, int n, sph_grid g,
@@ -87,20 +82,20 @@ __global__ void k_noalloc_ranges(const int* __restrict__ cell, int n, int* __res
   if (k == n - 1 || cell[k + 1] != c) end[c] = k;
 }
 
-// Once per device, with that device current: the device address of the scratch array.
+// The device address of the scratch array in the current device's current context.  In
+// host code the array's name is only a host-side stand-in, so the address is looked up,
+// and it is looked up on every call rather than cached: after cudaDeviceReset (which the
+// reference's main.cu calls) or in another context on the same device the array lives
+// at a new address.  The lookup is a host-side table query, cheap next to the launches.
+// The first lookup in a context loads this file's device code, which is where the array
+// is placed in device memory; no call allocates anything after that.
 sph_status scratch_for_current_device(int** out) {
-  int dev = -1;
-  if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= 256) return SPH_ERR_CUDA;
-  std::lock_guard<std::mutex> lock(g_setup_mutex);
-  if (!g_scratch_ptr[dev]) {
-    void* p = nullptr;
-    if (cudaGetSymbolAddress(&p, g_noalloc_scratch) != cudaSuccess || !p) {
-      cudaGetLastError();
-      return SPH_ERR_CUDA;
-    }
-    g_scratch_ptr[dev] = static_cast<int*>(p);
+  void* p = nullptr;
+  if (cudaGetSymbolAddress(&p, g_noalloc_scratch) != cudaSuccess || !p) {
+    cudaGetLastError();
+    return SPH_ERR_CUDA;
   }
-  *out = g_scratch_ptr[dev];
+  *out = static_cast<int*>(p);
   return SPH_OK;
 }
 

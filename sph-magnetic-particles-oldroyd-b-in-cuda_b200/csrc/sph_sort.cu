@@ -20,6 +20,9 @@ constexpr int kTile = kThreads * kItems;         // 4096
 constexpr int kMaxBits = 9;                      // up to 512 buckets per pass
 constexpr int kMaxBuckets = 1 << kMaxBits;
 constexpr int kScanChunk = 2048;                 // entries per scan block
+static_assert(kTile == kSortTile && kMaxBuckets == kSortMaxBuckets &&
+                  kScanChunk == kSortScanChunk,
+              "sort geometry must match the histogram size callers reserve (sort_hist_ints)");
 
 __global__ void __launch_bounds__(kThreads) k_radix_hist(const int* __restrict__ keys, int n,
                                                          int shift, int nbits, int ntiles,
@@ -169,10 +172,7 @@ __global__ void __launch_bounds__(kThreads)
 
 size_t sort_hist_len(int n, int key_bits) {
   (void)key_bits;
-  const int ntiles = (n + kTile - 1) / kTile;
-  const size_t m = (size_t)kMaxBuckets * (ntiles > 0 ? ntiles : 1);
-  const size_t nchunks = (m + kScanChunk - 1) / kScanChunk;
-  return m + nchunks + 32;
+  return sort_hist_ints(n);
 }
 
 // Sorts (key_by_gid[g], g) pairs by key; result in d.keys / d.vals.

@@ -194,6 +194,7 @@ __device__ __forceinline__ bool gemm_mainloop(const GemmArgs& g, uint8_t* smem, 
     fence_after_sync();
   };
   bool ok = true;
+  int issued = -1;  // the last chunk whose MMAs were committed
   if (nch > 0) fill(0);
   for (int c = 0; c < nch; ++c) {
     const int s = c & 1;
@@ -205,21 +206,28 @@ __device__ __forceinline__ bool gemm_mainloop(const GemmArgs& g, uint8_t* smem, 
                  (c > 0 || q > 0) ? 1 : 0);
       mma_commit(&bar[s]);
     }
+    issued = c;
     if (c + 1 < nch) {
       // stage s ^ 1 was read by the MMAs of chunk c - 1 (commit number (c - 1) / 2 of its
-      // barrier); every earlier commit of that barrier has been waited for
+      // barrier); every earlier commit of that barrier has been waited for.  Every thread
+      // waits (bounded) and the block takes one decision, so that all threads leave the
+      // loop together and meet the same barriers afterwards.
       if (c >= 1) {
-        ok = mbar_wait(&bar[s ^ 1], (uint32_t)(((c - 1) >> 1) & 1)) && ok;
+        ok = __syncthreads_and(mbar_wait(&bar[s ^ 1], (uint32_t)(((c - 1) >> 1) & 1)) ? 1 : 0) != 0;
         fence_after_sync();
       }
       if (!ok) break;
       fill(c + 1);
     }
   }
-  // the last commit completes after every MMA before it
-  if (ok && nch > 0) {
-    ok = mbar_wait(&bar[(nch - 1) & 1], (uint32_t)(((nch - 1) >> 1) & 1));
+  // The last commit completes after every MMA before it.  After a timeout this is the
+  // drain: a second bounded wait, so that the caller frees TMEM only once the MMAs that
+  // write it have finished (or this wait, too, has given up).  The previous commit of that
+  // barrier was waited for before the chunk was issued, so its parity is unambiguous.
+  if (issued >= 0) {
+    const bool done = mbar_wait(&bar[issued & 1], (uint32_t)((issued >> 1) & 1));
     fence_after_sync();
+    ok = ok && done;
   }
   return ok;
 }
