@@ -4,9 +4,12 @@
 Workload (the reference's headline configuration, 3D Couette flow): 128^3 lattice between
 y-walls (128 x 134 x 128 = 2,195,456 particles including the wall layers), L = 1,
 overlap = 3, V_wall = -0.5 / +0.5, rho = 1, c = 10, P0 = 0, eta = 0.1, zeta = 0,
-np = 100, kT = 0.01, tau = 1, dt = 2e-5; synthetic initial state (lattice, fluid at rest,
-c = I).  A step is the reference driver's step (main.cu:358-467): half-kick and drift,
-neighbour search, density, velocity gradient, forces, dc/dt, wall forces, half-kick.
+np = 100, kT = 0.01, tau = 1, dt = 2e-5; synthetic initial state: the lattice with c = I
+and every fluid velocity component drawn uniform in +-1e-3 c = +-0.01 from seed 2, given to
+both the engine and the reference as new_sim = 1 with an input_particles.in restart file
+(the only way the reference takes an initial velocity field).  A step is the reference
+driver's step (main.cu:358-467): half-kick and drift, neighbour search, density, velocity
+gradient, forces, dc/dt, wall forces, half-kick.
 
   python bench.py [--gpus N] [--steps K] [--warmup W] [--precision fp64|mixed]
   python bench.py --impl reference ...    # the reference's own CUDA build, same workload
@@ -58,7 +61,10 @@ import sph_input  # noqa: E402
 WORKLOAD = dict(N=(128, 128, 128), L=(1.0, 1.0, 1.0), dim=3, overlap=3.0, wall=1,
                 Vwall_bottom=-0.5, Vwall_top=0.5, rho=1.0, c=10.0, P0=0.0, eta=0.1, zeta=0.0,
                 np=100.0, kT=0.01, tau=1.0, dt=2e-5)
-WORKLOAD_NAME = "couette3d_128: 128^3 Oldroyd-B Couette flow between y-walls, 2,195,456 particles"
+WORKLOAD_NAME = ("couette3d_128: 128^3 Oldroyd-B Couette flow between y-walls, 2,195,456 "
+                 "particles, fluid velocities seeded uniform in +-1e-3 c")
+# seeded initial fluid velocities: uniform in [-VMAX, VMAX] per component, VMAX = 1e-3 c
+SEED, VMAX = 2, 1e-3 * 10.0
 METRIC = "particle-steps/s (128^3 Oldroyd-B Couette)"
 UNIT = "particle-steps/s"
 # Algorithmic bytes per particle-step of the whole step (four grid-wide phases, each
@@ -156,13 +162,20 @@ class ClockSampler:
 
 
 def write_workload(d, lattice=128):
-    """The Couette input; lattice < 128 gives a smaller box of the same physics, used only
-    for ncu captures that must stay small."""
-    path = os.path.join(d, "input")
+    """The Couette input (`input`, new_sim = 1) and its seeded start (`input_particles.in`)
+    in directory d; lattice < 128 gives a smaller box of the same physics, used only for ncu
+    captures that must stay small.  Returns the input path; the engine, the oracle and the
+    reference all read the same two files."""
+    import sph_b200
+
     spec = dict(WORKLOAD)
     spec["N"] = (lattice, lattice, lattice)
-    sph_input.write_input(path, **spec)
+    path, _, _ = sph_b200.write_seeded_start(d, spec, seed=SEED, vmax=VMAX)
     return path
+
+
+def particles_file(input_path):
+    return os.path.join(os.path.dirname(input_path), "input_particles.in")
 
 
 def cpu_baseline(workdir, steps=1):
@@ -170,7 +183,8 @@ def cpu_baseline(workdir, steps=1):
     import oracle
 
     cores = oracle.set_threads(os.cpu_count() or 1)
-    o = oracle.Oracle(write_workload(workdir))
+    inp = write_workload(workdir)
+    o = oracle.Oracle(inp, particles_file(inp))
     o.run(0)
     t0 = time.perf_counter()
     o.run(steps)
@@ -255,7 +269,8 @@ def run_ours(args, world, rank, local, dist):
 
     with tempfile.TemporaryDirectory() as wd:
         path = write_workload(wd, args.lattice)
-        sysm = sph_b200.System(path, precision=args.precision, device=local)
+        sysm = sph_b200.System(path, [particles_file(path)], precision=args.precision,
+                               device=local)
         n = sysm.N
         tuning = sysm.autotune() if not args.no_autotune else sysm.tuning()
         sysm.step(args.warmup)
@@ -304,7 +319,7 @@ def run_ours(args, world, rank, local, dist):
         "warmup": args.warmup, "ms_per_step": ms_max / args.steps, "higher_is_better": True,
         "scaling": "weak", "vs_baseline": None,
         "dtype": "f64" if args.precision == "fp64" else "f32 pairs / f64 state",
-        "data": "synthetic (lattice initial state)",
+        "data": "synthetic (lattice, fluid velocities seeded uniform in +-1e-3 c, seed %d)" % SEED,
         "config": {"workload": WORKLOAD_NAME, "particles": n, "precision": args.precision,
                    "parallelism": "replicas only" if world > 1 else "single box",
                    "launch_geometry": tuning,

@@ -209,11 +209,24 @@ sph_status sph_initial_forces(sph_ctx* ctx);
 
 /* main.cu:358-467 without output: nsteps x (VV1, search, m(t), forces, VV2).  Runs
    sph_initial_forces first if it has not run.  Asynchronous on the context's stream;
-   errors raised on the device are reported by the next sph_synchronize. */
+   errors raised on the device are reported by the next sph_synchronize (or by the next
+   call of any other function, which first waits for the open steps).  A step that finds a
+   problem stops there: its later kernels and all later steps do nothing, so the state is
+   never advanced on bad data.  A neighbour list found too short is not an error: the next
+   sph_synchronize grows the lists, finishes that step and runs the remaining steps.  A
+   position outside the grid or not finite is reported with the step it was found in, and
+   the state is left as that step's half-kick and drift made it; the step counter
+   (sph_get_info) gives the steps completed. */
 sph_status sph_step(sph_ctx* ctx, int nsteps);
 
-/* Waits for the context's stream and reports device-side error flags. */
+/* Waits for the context's stream and reports device-side error flags; resumes an sph_step
+   call whose lists had to grow (see sph_step). */
 sph_status sph_synchronize(sph_ctx* ctx);
+
+/* Neighbour-list statistics (no reference counterpart: the reference has no lists): the
+   capacity of a list row, the largest row the list builds have needed, and how many times
+   the lists have grown. */
+sph_status sph_neighbour_lists(sph_ctx* ctx, int* capacity, int* max_used, int* grown);
 
 /* -------------------------------------------------------------- state access */
 

@@ -42,6 +42,18 @@ sph_status sph_write_colloids(const char* path, int dim, int n, const double* co
 sph_status sph_write_gradv(const char* path, int dim, int n, const double* x, const double* y,
                            const double* z, const double* const* g);
 
+/* input_particles.in, the restart file that new_sim = 1 reads
+   (src/system_initialize_particles_old_sim.cpp:36,48): 2D rows "x y vx vy mass type cxx
+   cxy cyy", 3D rows "x y z vx vy vz mass type cxx cxy cyy cxz cyz czz", no index.  The
+   reference reads every column as float, so every value is rounded to float and written
+   with "%.9g", which reads back as exactly that float.  z, vz, cxz, cyz, czz are not read
+   in 2D. */
+sph_status sph_write_restart(const char* path, int dim, int n, const double* x, const double* y,
+                             const double* z, const double* vx, const double* vy,
+                             const double* vz, const double* mass, const int* type,
+                             const double* cxx, const double* cxy, const double* cyy,
+                             const double* cxz, const double* cyz, const double* czz);
+
 /* macro.dat (src/system_print_macro_vars.cu:34-47): "step KE" with "%f"; the file is
    created at step 0 and appended to otherwise. */
 sph_status sph_append_macro(const char* path, int step, double kin_energy);

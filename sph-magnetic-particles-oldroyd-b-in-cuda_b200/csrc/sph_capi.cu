@@ -47,6 +47,11 @@ struct sph_ctx {
   double last_ms = 0.0;
   int max_coll = 0;
   int cap_grown = 0;
+  // the last sph_step call, for resuming it after a full neighbour list was found in one of
+  // its steps: the step counter and buffer parity when it started, and the step it ends at
+  bool call_open = false;
+  long long call_step0 = 0, call_target = 0;
+  int call_parity0 = 0;
   sph_tuning tune = {32, 128};  // launch geometry (sph_set_tuning / sph_autotune)
 };
 
@@ -137,28 +142,44 @@ int derived_capacity(const std::vector<HostBox>& boxes, int dim) {
   return (cap + 7) / 8 * 8;
 }
 
+// Reads the device error flags and their record (err_info, kErrInfoLen ints) without
+// clearing them.  Blocks on the stream.
+bool read_device_status(sph_ctx* c, unsigned* st, int* info) {
+  return cudaMemcpyAsync(st, c->d.status, sizeof(unsigned), cudaMemcpyDeviceToHost,
+                         c->stream) == cudaSuccess &&
+         cudaMemcpyAsync(info, c->d.err_info, kErrInfoLen * sizeof(int), cudaMemcpyDeviceToHost,
+                         c->stream) == cudaSuccess &&
+         cudaStreamSynchronize(c->stream) == cudaSuccess;
+}
+
+long long failed_step(const int* info) {
+  return ((long long)info[kErrStepHi] << 32) | (long long)(unsigned)info[kErrStepLo];
+}
+
+// The status for a set of device flags; `where` names the step for failures inside a
+// multi-step call.
+sph_status status_of(sph_ctx* c, unsigned st, const int* info, const std::string& where) {
+  if (st & kStatNaN)
+    return fail(c, SPH_ERR_NAN, "non-finite particle position (global id " +
+                                    std::to_string(info[kErrBadId]) + ")" + where);
+  if (st & kStatCellRange)
+    return fail(c, SPH_ERR_CELL_RANGE, "particle hashed outside the cell grid (global id " +
+                                           std::to_string(info[kErrBadId]) + ")" + where);
+  if (st & kStatCapacity)
+    return fail(c, SPH_ERR_CAPACITY, "neighbour list capacity " + std::to_string(c->d.cap) +
+                                         " exceeded (" + std::to_string(info[kErrMaxCount]) +
+                                         " needed)" + where);
+  return SPH_OK;
+}
+
 // Reads and clears the device error flags.  Blocks on the stream.
 sph_status check_device(sph_ctx* c) {
   unsigned st = 0;
-  int info[2] = {0, 0};
-  if (cudaMemcpyAsync(&st, c->d.status, sizeof(unsigned), cudaMemcpyDeviceToHost, c->stream) !=
-          cudaSuccess ||
-      cudaMemcpyAsync(info, c->d.err_info, 2 * sizeof(int), cudaMemcpyDeviceToHost, c->stream) !=
-          cudaSuccess ||
-      cudaStreamSynchronize(c->stream) != cudaSuccess)
-    return cuda_fail(c, "device status");
+  int info[kErrInfoLen] = {0};
+  if (!read_device_status(c, &st, info)) return cuda_fail(c, "device status");
   if (st == 0) return SPH_OK;
   cudaMemsetAsync(c->d.status, 0, sizeof(unsigned), c->stream);
-  if (st & kStatNaN)
-    return fail(c, SPH_ERR_NAN, "non-finite particle position (global id " +
-                                    std::to_string(info[0]) + ")");
-  if (st & kStatCellRange)
-    return fail(c, SPH_ERR_CELL_RANGE, "particle hashed outside the cell grid (global id " +
-                                           std::to_string(info[0]) + ")");
-  if (st & kStatCapacity)
-    return fail(c, SPH_ERR_CAPACITY, "neighbour list capacity " + std::to_string(c->d.cap) +
-                                         " exceeded (" + std::to_string(info[1]) + " needed)");
-  return SPH_OK;
+  return status_of(c, st, info, "");
 }
 
 void drop_graphs(sph_ctx* c) {
@@ -271,18 +292,32 @@ sph_status host_moment(sph_ctx* c, long long step) {
   return SPH_OK;
 }
 
+// Lists too short for the current positions: grow them to the largest row the list build
+// saw and build them again (with the colloid coarse grid, which the failed search skipped),
+// until they fit.  The device flags are clear on entry.
+sph_status regrow_lists(sph_ctx* c) {
+  for (int round = 0; round < 4; ++round) {
+    int need = 0;
+    if (cudaMemcpy(&need, c->d.err_info + kErrMaxCount, sizeof(int), cudaMemcpyDeviceToHost) !=
+        cudaSuccess)
+      return cuda_fail(c, "list statistics");
+    sph_status s = grow_capacity(c, need);
+    if (s != SPH_OK) return s;
+    cudaMemsetAsync(c->d.err_info + kErrMaxCount, 0, sizeof(int), c->stream);
+    Launch L = launcher(c);
+    if (launch_build_lists_dim(L, c->dim)) return cuda_fail(c, "rebuild lists");
+    if (c->d.ncoll > 0 && launch_colloid_cells_n(L, c->nboxes, c->max_coll))
+      return cuda_fail(c, "rebuild colloid cells");
+    s = check_device(c);
+    if (s != SPH_ERR_CAPACITY) return s;
+  }
+  return fail(c, SPH_ERR_CAPACITY, "neighbour lists still too short after growing them");
+}
+
 sph_status search_checked(sph_ctx* c) {
   if (ph_search(c)) return cuda_fail(c, "neighbours_search");
   sph_status s = check_device(c);
-  if (s == SPH_ERR_CAPACITY) {
-    int info[2];
-    cudaMemcpy(info, c->d.err_info, sizeof(info), cudaMemcpyDeviceToHost);
-    s = grow_capacity(c, info[1]);
-    if (s != SPH_OK) return s;
-    cudaMemsetAsync(c->d.err_info + 1, 0, sizeof(int), c->stream);
-    if (launch_build_lists_dim(launcher(c), c->dim)) return cuda_fail(c, "rebuild lists");
-    s = check_device(c);
-  }
+  if (s == SPH_ERR_CAPACITY) s = regrow_lists(c);
   return s;
 }
 
@@ -327,6 +362,91 @@ sph_status capture_graphs(sph_ctx* c) {
     c->launches = before;
   }
   return SPH_OK;
+}
+
+// Launches n whole steps: CUDA-graph replays (captured first if needed) or direct launches.
+sph_status run_steps(sph_ctx* c, long long n) {
+  if (n <= 0) return SPH_OK;
+  if (c->use_graph && !c->graph[0]) {
+    sph_status s = capture_graphs(c);
+    if (s != SPH_OK) return s;
+  }
+  for (long long k = 0; k < n; ++k) {
+    if (c->use_graph) {
+      if (cudaGraphLaunch(c->graph[c->parity], c->stream) != cudaSuccess)
+        return cuda_fail(c, "graph launch");
+      swap_state(c, false);
+      c->launches += c->graph_kernels;
+    } else if (ph_step(c)) {
+      return cuda_fail(c, "step");
+    }
+    c->host_step++;
+  }
+  c->forces_live = true;
+  c->pos_dirty = false;
+  return SPH_OK;
+}
+
+// Waits for the open sph_step call(s) and checks their steps.  A step that found its
+// neighbour lists too short stopped every kernel after its list build (and every later
+// step); here the lists grow, the step is finished from its list build, and the remaining
+// steps run, until the call's last step is done.  A position outside the grid or not finite
+// is reported with the step it was found in; the state is then the one that step left
+// after its half-kick and drift (the step counter says how many steps were completed).
+sph_status settle_call(sph_ctx* c) {
+  for (int round = 0;; ++round) {
+    unsigned st = 0;
+    int info[kErrInfoLen] = {0};
+    if (!read_device_status(c, &st, info)) {
+      c->call_open = false;
+      return cuda_fail(c, "device status");
+    }
+    if (st == 0) {
+      c->call_open = false;
+      return SPH_OK;
+    }
+    cudaMemsetAsync(c->d.status, 0, sizeof(unsigned), c->stream);
+    // the host's view of the stopped call: completed steps and the buffer parity of the
+    // reorders that did run (the failing step's own reorder ran if its list build reported)
+    const long long done = failed_step(info);
+    const int phase = info[kErrPhase];
+    const long long reorders = (done - c->call_step0) + (phase == kPhaseLists ? 1 : 0);
+    const int parity = c->call_parity0 ^ (int)(reorders & 1);
+    if (c->parity != parity) swap_state(c, false);
+    c->host_step = done;
+    const std::string where = " in step " + std::to_string(done + 1);
+    if (!(st == kStatCapacity && phase == kPhaseLists && round < 8)) {
+      c->call_open = false;
+      c->forces_live = false;
+      c->pos_dirty = true;
+      c->gradv_valid = false;
+      return status_of(c, st, info,
+                       where + "; the state is that step's after its half-kick and drift");
+    }
+    sph_status s = regrow_lists(c);
+    if (s == SPH_OK && (launch_advance_time(launcher(c), 0) || ph_forces(c, true) ||
+                        ph_vv2(c, true)))
+      s = cuda_fail(c, "resumed step");
+    if (s != SPH_OK) {
+      c->call_open = false;
+      c->pos_dirty = true;
+      return s;
+    }
+    c->host_step = done + 1;
+    c->forces_live = true;
+    c->pos_dirty = false;
+    c->call_step0 = c->host_step;
+    c->call_parity0 = c->parity;
+    s = run_steps(c, c->call_target - c->host_step);
+    if (s != SPH_OK) {
+      c->call_open = false;
+      return s;
+    }
+    if (cudaStreamSynchronize(c->stream) != cudaSuccess) {
+      c->call_open = false;
+      return cuda_fail(c, "synchronize");
+    }
+  }
 }
 
 void free_ctx(sph_ctx* c) {
@@ -596,7 +716,8 @@ sph_status sph_create_ensemble(int nboxes, const sph_input* inputs,
   ok = ok && dalloc(c, &d.ccell, ncoll) && dalloc(c, &d.cindex, ncoll);
   ok = ok && dalloc(c, &d.ccell_start, ncc) && dalloc(c, &d.ccell_end, ncc);
   ok = ok && dalloc(c, &d.mag, 3 * nboxes) && dalloc(c, &d.ke, nboxes);
-  ok = ok && dalloc(c, &d.step, 1) && dalloc(c, &d.status, 1) && dalloc(c, &d.err_info, 2);
+  ok = ok && dalloc(c, &d.step, 1) && dalloc(c, &d.status, 1) &&
+       dalloc(c, &d.err_info, kErrInfoLen);
   ok = ok && dalloc(c, &c->scratch, Np) && dalloc(c, &c->iscratch, Np);
   c->sort.hist_len = (int)sort_hist_len(Ntot, c->key_bits);
   ok = ok && dalloc(c, &c->sort.hist, (size_t)c->sort.hist_len);
@@ -798,14 +919,22 @@ sph_status sph_get_info(const sph_ctx* c, int box, sph_info* o) {
 #define CTX_GUARD(c)                  \
   if (!(c)) return SPH_ERR_STATE;     \
   cudaSetDevice((c)->device);
+// ... and, for every call except sph_step and sph_synchronize, first settles an open
+// sph_step call (waits for it, resumes it after a list overflow or reports its failure)
+#define CTX_SETTLED(c)                                  \
+  CTX_GUARD(c);                                         \
+  if ((c)->call_open) {                                 \
+    const sph_status settle_status_ = settle_call(c);   \
+    if (settle_status_ != SPH_OK) return settle_status_; \
+  }
 
 sph_status sph_neighbours_search(sph_ctx* c) {
-  CTX_GUARD(c);
+  CTX_SETTLED(c);
   return search_checked(c);
 }
 
 sph_status sph_calculate_density(sph_ctx* c) {
-  CTX_GUARD(c);
+  CTX_SETTLED(c);
   sph_status s = ensure_lists(c);
   if (s != SPH_OK) return s;
   if (launch_density_dim(launcher(c), c->dim)) return cuda_fail(c, "calculate_density");
@@ -813,13 +942,13 @@ sph_status sph_calculate_density(sph_ctx* c) {
 }
 
 sph_status sph_calculate_pressure(sph_ctx* c) {
-  CTX_GUARD(c);
+  CTX_SETTLED(c);
   if (launch_pressure(launcher(c))) return cuda_fail(c, "calculate_pressure");
   return SPH_OK;
 }
 
 sph_status sph_calculate_vel_gradient(sph_ctx* c) {
-  CTX_GUARD(c);
+  CTX_SETTLED(c);
   sph_status s = ensure_lists(c);
   if (s != SPH_OK) return s;
   // the pair pass reads the neighbour records, refreshed from the current state
@@ -830,7 +959,7 @@ sph_status sph_calculate_vel_gradient(sph_ctx* c) {
 }
 
 sph_status sph_calculate_forces(sph_ctx* c, const double* m) {
-  CTX_GUARD(c);
+  CTX_SETTLED(c);
   sph_status s = ensure_lists(c);
   if (s != SPH_OK) return s;
   s = m ? upload_moment(c, m) : host_moment(c, c->host_step + (c->in_step ? 1 : 0));
@@ -854,19 +983,19 @@ sph_status sph_calculate_forces(sph_ctx* c, const double* m) {
 }
 
 sph_status sph_calculate_external_forces(sph_ctx* c) {
-  CTX_GUARD(c);
+  CTX_SETTLED(c);
   if (launch_ext_force(launcher(c))) return cuda_fail(c, "external forces");
   return SPH_OK;
 }
 
 sph_status sph_calculate_force_walls(sph_ctx* c) {
-  CTX_GUARD(c);
+  CTX_SETTLED(c);
   if (launch_wall_forces(launcher(c))) return cuda_fail(c, "force_walls");
   return SPH_OK;
 }
 
 sph_status sph_calculate_force_colloids(sph_ctx* c, const double* m) {
-  CTX_GUARD(c);
+  CTX_SETTLED(c);
   sph_status s = m ? upload_moment(c, m) : host_moment(c, c->host_step + (c->in_step ? 1 : 0));
   if (s != SPH_OK) return s;
   if (c->pos_dirty) {
@@ -880,14 +1009,14 @@ sph_status sph_calculate_force_colloids(sph_ctx* c, const double* m) {
 }
 
 sph_status sph_vv_step1(sph_ctx* c) {
-  CTX_GUARD(c);
+  CTX_SETTLED(c);
   if (ph_vv1(c)) return cuda_fail(c, "V_Verlet_step1");
   c->in_step = true;
   return SPH_OK;
 }
 
 sph_status sph_vv_step2(sph_ctx* c) {
-  CTX_GUARD(c);
+  CTX_SETTLED(c);
   if (ph_vv2(c)) return cuda_fail(c, "V_Verlet_step2");
   c->host_step++;
   c->in_step = false;
@@ -895,7 +1024,7 @@ sph_status sph_vv_step2(sph_ctx* c) {
 }
 
 sph_status sph_initial_forces(sph_ctx* c) {
-  CTX_GUARD(c);
+  CTX_SETTLED(c);
   return do_initial(c);
 }
 
@@ -903,29 +1032,25 @@ sph_status sph_step(sph_ctx* c, int nsteps) {
   CTX_GUARD(c);
   if (nsteps < 0) return SPH_ERR_STATE;
   if (!c->initial_done) {
+    if (c->call_open) {
+      sph_status s = settle_call(c);
+      if (s != SPH_OK) return s;
+    }
     sph_status s = do_initial(c);
     if (s != SPH_OK) return s;
   }
   if (c->in_step) return fail(c, SPH_ERR_STATE, "sph_step inside a half-finished step");
   if (nsteps == 0) return SPH_OK;
-  if (c->use_graph && !c->graph[0]) {
-    sph_status s = capture_graphs(c);
-    if (s != SPH_OK) return s;
+  // calls made without a synchronize in between form one open call
+  if (!c->call_open) {
+    c->call_open = true;
+    c->call_step0 = c->host_step;
+    c->call_parity0 = c->parity;
   }
   cudaEventRecord(c->ev0, c->stream);
-  for (int k = 0; k < nsteps; ++k) {
-    if (c->use_graph) {
-      if (cudaGraphLaunch(c->graph[c->parity], c->stream) != cudaSuccess)
-        return cuda_fail(c, "graph launch");
-      swap_state(c, false);
-      c->launches += c->graph_kernels;
-    } else if (ph_step(c)) {
-      return cuda_fail(c, "step");
-    }
-    c->host_step++;
-  }
-  c->forces_live = true;
-  c->pos_dirty = false;
+  sph_status s = run_steps(c, nsteps);
+  c->call_target = c->host_step;
+  if (s != SPH_OK) return s;
   cudaEventRecord(c->ev1, c->stream);
   c->events_recorded = true;
   return SPH_OK;
@@ -939,14 +1064,26 @@ sph_status sph_synchronize(sph_ctx* c) {
     if (cudaEventElapsedTime(&ms, c->ev0, c->ev1) == cudaSuccess) c->last_ms = ms;
     c->events_recorded = false;
   }
-  sph_status s = check_device(c);
+  sph_status s = c->call_open ? settle_call(c) : check_device(c);
   if (s == SPH_OK) {
-    int info[2];
-    cudaMemcpy(info, c->d.err_info, sizeof(info), cudaMemcpyDeviceToHost);
+    int used = 0;
+    cudaMemcpy(&used, c->d.err_info + kErrMaxCount, sizeof(int), cudaMemcpyDeviceToHost);
     // keep headroom: grow the lists (and recapture) once 90% of the capacity is in use
-    if (info[1] > (9 * c->d.cap) / 10) s = grow_capacity(c, info[1]);
+    if (used > (9 * c->d.cap) / 10) s = grow_capacity(c, used);
   }
   return s;
+}
+
+sph_status sph_neighbour_lists(sph_ctx* c, int* capacity, int* max_used, int* grown) {
+  CTX_SETTLED(c);
+  int used = 0;
+  if (cudaMemcpy(&used, c->d.err_info + kErrMaxCount, sizeof(int), cudaMemcpyDeviceToHost) !=
+      cudaSuccess)
+    return cuda_fail(c, "list statistics");
+  if (capacity) *capacity = c->d.cap;
+  if (max_used) *max_used = used;
+  if (grown) *grown = c->cap_grown;
+  return SPH_OK;
 }
 
 sph_status sph_last_step_ms(sph_ctx* c, double* ms) {
@@ -969,7 +1106,7 @@ const char* sph_phase_name(int k) {
 }
 
 sph_status sph_profile_phases(sph_ctx* c, int nsteps, double* ms) {
-  CTX_GUARD(c);
+  CTX_SETTLED(c);
   if (!ms || nsteps <= 0) return SPH_ERR_STATE;
   if (!c->initial_done) {
     sph_status s = do_initial(c);
@@ -1035,7 +1172,7 @@ sph_status sph_profile_phases(sph_ctx* c, int nsteps, double* ms) {
 
 // ---- state access ----
 sph_status sph_read_field_device(sph_ctx* c, int field, double* dev_out) {
-  CTX_GUARD(c);
+  CTX_SETTLED(c);
   if (field < 0 || field >= SPH_NUM_PARTICLE_FIELDS || !dev_out) return SPH_ERR_STATE;
   if (field >= SPH_GXX && field <= SPH_GZZ && !c->gradv_valid) {
     if (sph_calculate_vel_gradient(c) != SPH_OK) return SPH_ERR_CUDA;
@@ -1045,7 +1182,7 @@ sph_status sph_read_field_device(sph_ctx* c, int field, double* dev_out) {
 }
 
 sph_status sph_read_field(sph_ctx* c, int field, double* host_out) {
-  CTX_GUARD(c);
+  CTX_SETTLED(c);
   if (!host_out) return SPH_ERR_STATE;
   sph_status s = sph_read_field_device(c, field, c->scratch);
   if (s != SPH_OK) return s;
@@ -1057,7 +1194,7 @@ sph_status sph_read_field(sph_ctx* c, int field, double* host_out) {
 }
 
 sph_status sph_write_field(sph_ctx* c, int field, const double* host_in) {
-  CTX_GUARD(c);
+  CTX_SETTLED(c);
   if (field < 0 || field >= SPH_NUM_PARTICLE_FIELDS || !host_in) return SPH_ERR_STATE;
   if (cudaMemcpyAsync(c->scratch, host_in, (size_t)c->d.Ntot * sizeof(double),
                       cudaMemcpyHostToDevice, c->stream) != cudaSuccess)
@@ -1070,7 +1207,7 @@ sph_status sph_write_field(sph_ctx* c, int field, const double* host_in) {
 }
 
 sph_status sph_read_type(sph_ctx* c, int* host_out) {
-  CTX_GUARD(c);
+  CTX_SETTLED(c);
   if (!host_out) return SPH_ERR_STATE;
   if (launch_gather_int(launcher(c), c->d.tinfo, c->iscratch)) return cuda_fail(c, "read_type");
   std::vector<int> t(c->d.Ntot);
@@ -1083,7 +1220,7 @@ sph_status sph_read_type(sph_ctx* c, int* host_out) {
 }
 
 sph_status sph_read_colloid_field(sph_ctx* c, int field, double* host_out) {
-  CTX_GUARD(c);
+  CTX_SETTLED(c);
   if (field < 0 || field >= SPH_NUM_COLLOID_FIELDS || !host_out) return SPH_ERR_STATE;
   if (c->d.ncoll == 0) return SPH_OK;
   if (cudaMemcpyAsync(host_out, c->d.cs + (size_t)field * c->d.ncoll,
@@ -1095,7 +1232,7 @@ sph_status sph_read_colloid_field(sph_ctx* c, int field, double* host_out) {
 }
 
 sph_status sph_read_wall_forces(sph_ctx* c, double* host_out) {
-  CTX_GUARD(c);
+  CTX_SETTLED(c);
   if (!host_out) return SPH_ERR_STATE;
   std::vector<double> wf(3 * (size_t)std::max(c->d.nwallseg, 1));
   if (c->d.nwallseg > 0 &&
@@ -1113,7 +1250,7 @@ sph_status sph_read_wall_forces(sph_ctx* c, double* host_out) {
 
 sph_status sph_export_cells(sph_ctx* c, int* particle_cell, int* particle_index,
                             int* cell_start, int* cell_end) {
-  CTX_GUARD(c);
+  CTX_SETTLED(c);
   const BoxParams& p = c->boxes[0].p;
   cudaStream_t st = c->stream;
   bool ok = true;
@@ -1130,7 +1267,7 @@ sph_status sph_export_cells(sph_ctx* c, int* particle_cell, int* particle_index,
 
 sph_status sph_export_colloid_cells(sph_ctx* c, int* coll_cell, int* coll_index,
                                     int* coll_cell_start, int* coll_cell_end) {
-  CTX_GUARD(c);
+  CTX_SETTLED(c);
   const BoxParams& p = c->boxes[0].p;
   if (p.N_colloids == 0) return SPH_OK;
   cudaStream_t st = c->stream;
@@ -1147,7 +1284,7 @@ sph_status sph_export_colloid_cells(sph_ctx* c, int* coll_cell, int* coll_index,
 }
 
 sph_status sph_kinetic_energy(sph_ctx* c, double* host_out) {
-  CTX_GUARD(c);
+  CTX_SETTLED(c);
   if (!host_out) return SPH_ERR_STATE;
   if (launch_kinetic_energy(launcher(c), c->ke_partial)) return cuda_fail(c, "kinetic_energy");
   if (cudaMemcpyAsync(host_out, c->d.ke, (size_t)c->nboxes * sizeof(double),
@@ -1159,7 +1296,7 @@ sph_status sph_kinetic_energy(sph_ctx* c, double* host_out) {
 
 // ---- observables ----
 sph_status sph_observe(sph_ctx* c) {
-  CTX_GUARD(c);
+  CTX_SETTLED(c);
   if (c->in_step) return fail(c, SPH_ERR_STATE, "observe inside a half-finished step");
   if (!c->initial_done) {
     sph_status s = do_initial(c);
@@ -1172,7 +1309,7 @@ sph_status sph_observe(sph_ctx* c) {
 }
 
 sph_status sph_observables(sph_ctx* c, double* host_out, long long* nsamples) {
-  CTX_GUARD(c);
+  CTX_SETTLED(c);
   if (!host_out) return SPH_ERR_STATE;
   const size_t n = (size_t)SPH_NUM_OBS * c->nboxes;
   if (cudaMemcpyAsync(host_out, c->obs_acc, n * sizeof(double), cudaMemcpyDeviceToHost,
@@ -1186,7 +1323,7 @@ sph_status sph_observables(sph_ctx* c, double* host_out, long long* nsamples) {
 }
 
 sph_status sph_reset_observables(sph_ctx* c) {
-  CTX_GUARD(c);
+  CTX_SETTLED(c);
   if (cudaMemsetAsync(c->obs_acc, 0, (size_t)SPH_NUM_OBS * c->nboxes * sizeof(double),
                       c->stream) != cudaSuccess)
     return cuda_fail(c, "reset_observables");
@@ -1211,7 +1348,7 @@ struct CkptHeader {
 }  // namespace
 
 sph_status sph_save_checkpoint(sph_ctx* c, const char* path) {
-  CTX_GUARD(c);
+  CTX_SETTLED(c);
   if (!path) return SPH_ERR_STATE;
   if (c->in_step) return fail(c, SPH_ERR_STATE, "checkpoint inside a half-finished step");
   sph_status s = sph_synchronize(c);
@@ -1252,7 +1389,7 @@ sph_status sph_save_checkpoint(sph_ctx* c, const char* path) {
 }
 
 sph_status sph_load_checkpoint(sph_ctx* c, const char* path) {
-  CTX_GUARD(c);
+  CTX_SETTLED(c);
   if (!path) return SPH_ERR_STATE;
   if (c->in_step) return fail(c, SPH_ERR_STATE, "checkpoint inside a half-finished step");
   FILE* f = std::fopen(path, "rb");
@@ -1412,7 +1549,7 @@ sph_status sph_get_tuning(const sph_ctx* c, sph_tuning* out) {
 }
 
 sph_status sph_set_tuning(sph_ctx* c, const sph_tuning* t) {
-  CTX_GUARD(c);
+  CTX_SETTLED(c);
   if (!t || !tuning_ok(*t)) return fail(c, SPH_ERR_STATE, "unsupported launch geometry");
   c->tune = *t;
   drop_graphs(c);  // the captured steps carry the old geometry
@@ -1420,7 +1557,7 @@ sph_status sph_set_tuning(sph_ctx* c, const sph_tuning* t) {
 }
 
 sph_status sph_autotune(sph_ctx* c, const char* cache_path, sph_tuning* chosen) {
-  CTX_GUARD(c);
+  CTX_SETTLED(c);
   if (c->in_step) return fail(c, SPH_ERR_STATE, "autotune inside a half-finished step");
   const std::string key = tune_key(c);
   sph_tuning t;

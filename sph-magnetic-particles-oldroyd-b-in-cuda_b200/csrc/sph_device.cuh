@@ -134,9 +134,29 @@ __device__ __forceinline__ bool own_cell(const BoxParams& p, double x, double y,
   return true;
 }
 
-__device__ __forceinline__ void raise_status(const Dev& d, unsigned bit, int info) {
-  unsigned old = atomicOr(d.status, bit);
-  if (!(old & bit) && bit != kStatCapacity) atomicExch(&d.err_info[0], info);
+// Reports a failure.  The first report of any kind also records the step counter and the
+// phase; the first report of a bad position records the particle's global id.
+__device__ __forceinline__ void raise_status(const Dev& d, unsigned bit, int info, int phase) {
+  const unsigned old = atomicOr(d.status, bit);
+  if (!(old & bit) && bit != kStatCapacity) atomicExch(&d.err_info[kErrBadId], info);
+  if (!(old & kStatAbortMask)) {
+    const long long s = *d.step;
+    d.err_info[kErrStepLo] = (int)(s & 0xffffffffLL);
+    d.err_info[kErrStepHi] = (int)(s >> 32);
+    d.err_info[kErrPhase] = phase;
+  }
+}
+
+// True once a kernel before this one reported a failure: the step's state-changing kernels
+// then return at entry.  The flag word is read past L1 (it is written by atomics in L2).  In
+// kernels whose warps cooperate, lane 0's reading is taken by the whole warp.
+__device__ __forceinline__ bool step_aborted(const Dev& d) {
+  return (*(volatile const unsigned*)d.status & kStatAbortMask) != 0u;
+}
+__device__ __forceinline__ bool step_aborted_warp(const Dev& d) {
+  unsigned v = 0u;
+  if ((threadIdx.x & 31) == 0) v = *(volatile const unsigned*)d.status;
+  return (__shfl_sync(0xffffffffu, v, 0) & kStatAbortMask) != 0u;
 }
 
 

@@ -17,11 +17,27 @@ namespace sph {
 constexpr int kTypeBits = 12;
 constexpr int kTypeMask = (1 << kTypeBits) - 1;
 
-// Device error flags (bit set in Ctx::d_status by any kernel that detects the condition).
+// Device error flags (bit set in Dev::status by any kernel that detects the condition).
+// Once any of them is set, every state-changing kernel of the step returns at entry, so a
+// failure found in step k of a multi-step (graph-replayed) call leaves the state where step
+// k found it; the first report records the step counter and the phase (Dev::err_info).
 enum StatusBits : unsigned {
   kStatCellRange = 1u, // hash outside the grid (reference traps: kernel_cell_ranges.cu:20-23)
   kStatNaN = 2u,       // non-finite position
   kStatCapacity = 4u,  // neighbour list full
+  kStatAbortMask = 7u,
+};
+// Phase that made the first report: the hash (state not yet reordered in that step) or the
+// list build (state reordered, lists incomplete).
+enum FailPhase : int { kPhaseNone = 0, kPhaseHash = 1, kPhaseLists = 2 };
+// Dev::err_info entries.
+enum ErrInfo : int {
+  kErrBadId = 0,     // global id of the first particle outside the grid / not finite
+  kErrMaxCount = 1,  // largest neighbour-list row seen since the last reset
+  kErrStepLo = 2,    // device step counter (completed steps) at the first report, low word
+  kErrStepHi = 3,    // ... high word
+  kErrPhase = 4,     // FailPhase of the first report
+  kErrInfoLen = 8,
 };
 
 // Per-box constants.  Everything the reference keeps in __constant__ memory
@@ -189,7 +205,7 @@ struct Dev {
   int nkechunks;
   long long* step;     // device step counter (graph replays)
   unsigned* status;
-  int* err_info;       // [0] first bad slot, [1] largest neighbour count seen
+  int* err_info;       // kErrInfoLen ints, see ErrInfo
   int grad_all;        // fused pair pass: velocity gradient of every particle, not only fluid
   int fold_vv2;        // fused pair pass: also the step's second half-kick of fluid particles
 };

@@ -79,14 +79,27 @@ int fixed8(double x, char* out) {
   return (int)(p - out);
 }
 
-// One output column: a double array, or the int array printed with "%d".
+// One output column: a double array (printed with "%.8f"), or the int array printed with
+// "%d"; with g9, the double array rounded to float and printed with "%.9g", the shortest
+// form that reads back as the same float for every value.
 struct Col {
   const double* d;
   const int* i;
+  bool g9 = false;
 };
 
-// Writes rows "idx c0 c1 ... <end>" for idx = 0..n-1, formatted in parallel chunks.
-sph_status write_rows(const char* path, int n, const std::vector<Col>& cols, const char* end) {
+inline int put_col(const Col& c, int64_t r, char* p) {
+  if (c.g9) {
+    const double v = c.d ? (double)(float)c.d[r] : (double)(float)c.i[r];
+    return std::snprintf(p, 32, "%.9g", v);
+  }
+  return c.d ? fixed8(c.d[r], p) : put_int(c.i[r], p);
+}
+
+// Writes rows "idx c0 c1 ... <end>" for idx = 0..n-1 (without the index, "c0 c1 ... <end>"),
+// formatted in parallel chunks.
+sph_status write_rows(const char* path, int n, const std::vector<Col>& cols, const char* end,
+                      bool index = true) {
   FILE* f = std::fopen(path, "w");
   if (!f) return SPH_ERR_IO;
   const int64_t chunk = 32768;
@@ -110,10 +123,12 @@ sph_status write_rows(const char* path, int n, const std::vector<Col>& cols, con
       for (int64_t r = a; r < b; ++r) {
         if (off + row_max > s.size()) s.resize(std::max(2 * s.size(), off + row_max));
         char* p = &s[off];
-        p += put_int((int)r, p);
+        if (index) p += put_int((int)r, p);
+        bool first = !index;
         for (const Col& c : cols) {
-          *p++ = ' ';
-          p += c.d ? fixed8(c.d[r], p) : put_int(c.i[r], p);
+          if (!first) *p++ = ' ';
+          first = false;
+          p += put_col(c, r, p);
         }
         std::memcpy(p, end, endlen);
         p += endlen;
@@ -199,6 +214,23 @@ sph_status sph_write_gradv(const char* path, int dim, int n, const double* x, co
   for (const Col& k : c)
     if (!k.d) return SPH_ERR_STATE;
   return write_rows(path, n, c, "\n");
+}
+
+sph_status sph_write_restart(const char* path, int dim, int n, const double* x, const double* y,
+                             const double* z, const double* vx, const double* vy,
+                             const double* vz, const double* mass, const int* type,
+                             const double* cxx, const double* cxy, const double* cyy,
+                             const double* cxz, const double* cyz, const double* czz) {
+  if (!path || !dim_ok(dim) || n < 0) return SPH_ERR_STATE;
+  auto g = [](const double* d) { return Col{d, nullptr, true}; };
+  const Col t{nullptr, type, true};
+  const std::vector<Col> c =
+      dim == 2 ? std::vector<Col>{g(x), g(y), g(vx), g(vy), g(mass), t, g(cxx), g(cxy), g(cyy)}
+               : std::vector<Col>{g(x),   g(y),   g(z),   g(vx),  g(vy),  g(vz),  g(mass),
+                                  t,      g(cxx), g(cxy), g(cyy), g(cxz), g(cyz), g(czz)};
+  for (const Col& k : c)
+    if (!k.d && !k.i) return SPH_ERR_STATE;
+  return write_rows(path, n, c, "\n", false);
 }
 
 sph_status sph_append_macro(const char* path, int step, double kin_energy) {

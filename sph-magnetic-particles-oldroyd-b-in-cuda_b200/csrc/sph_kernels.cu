@@ -25,6 +25,7 @@ namespace sph {
 __global__ void k_vv1_particles(Dev d) {
   int i = blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= d.Ntot) return;
+  if (step_aborted(d)) return;
   int ti = d.tinfo[i];
   int t = type_of(ti);
   if (t > 2) return;  // colloid particles are placed by k_vv1_colloids
@@ -72,6 +73,7 @@ __global__ void k_vv1_particles(Dev d) {
 __global__ void k_vv2_particles(Dev d) {
   int i = blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= d.Ntot) return;
+  if (step_aborted(d)) return;
   int ti = d.tinfo[i];
   if (type_of(ti) != 0) return;
   const BoxParams& p = d.box[box_of(ti)];
@@ -100,6 +102,7 @@ __device__ __forceinline__ void qmul(const double* c, const double* e, double* r
 __global__ void k_vv1_colloids(Dev d) {
   const int c = blockIdx.x;
   if (c >= d.ncoll) return;
+  if (step_aborted(d)) return;
   const BoxParams& p = d.box[d.coll_box[c]];
   if (p.coll_move != 0) return;
   __shared__ double rot[4];  // 2D: cos, sin; 3D: quaternion
@@ -212,6 +215,7 @@ __global__ void k_vv1_colloids(Dev d) {
 __global__ void k_vv2_colloids(Dev d) {
   int c = blockIdx.x * blockDim.x + threadIdx.x;
   if (c >= d.ncoll) return;
+  if (step_aborted(d)) return;
   const BoxParams& p = d.box[d.coll_box[c]];
   if (p.coll_move != 0) return;
   const int nc = d.ncoll;
@@ -233,12 +237,13 @@ __global__ void k_vv2_colloids(Dev d) {
 __global__ void k_hash(Dev d) {
   int i = blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= d.Ntot) return;
+  if (step_aborted(d)) return;
   int ti = d.tinfo[i];
   const BoxParams& p = d.box[box_of(ti)];
   double4 x = d.pos[i];
   int c = hash_cell(p, x.x, x.y, x.z);
   if (c < 0) {
-    raise_status(d, c == -2 ? kStatNaN : kStatCellRange, d.gid[i]);
+    raise_status(d, c == -2 ? kStatNaN : kStatCellRange, d.gid[i], kPhaseHash);
     c = 0;  // keep the sort in bounds; the step is reported as failed
   }
   d.key_by_gid[d.gid[i]] = p.cell0 + c;
@@ -252,6 +257,7 @@ template <bool MIXED, bool PERMUTE_F>
 __global__ void k_reorder(Dev d) {
   int k = blockIdx.x * blockDim.x + threadIdx.x;
   if (k >= d.Ntot) return;
+  if (step_aborted(d)) return;
   const int g = d.vals[k];
   const int o = d.inv[g];
   const int Np = d.Npad;
@@ -388,6 +394,7 @@ __global__ void __launch_bounds__(kListWarps * 32) k_build_lists(Dev d) {
   __shared__ unsigned hmask[kListWarps][kMaxCh][32];
   __shared__ int hbase[kListWarps][kMaxCh][2];
   const int w = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  if (step_aborted_warp(d)) return;
   const int sub = lane / TPC, gl = lane % TPC;  // group within the warp, lane within the group
   float* stx = &stage_x[w][sub * TPC];
   float* sty = &stage_y[w][sub * TPC];
@@ -433,7 +440,7 @@ __global__ void __launch_bounds__(kListWarps * 32) k_build_lists(Dev d) {
         // not finite or far outside the box: already reported by the hash; no neighbours
         lost = true;
         const bool finite = isfinite(x.x) && isfinite(x.y) && isfinite(x.z);
-        raise_status(d, finite ? kStatCellRange : kStatNaN, d.gid[i]);
+        raise_status(d, finite ? kStatCellRange : kStatNaN, d.gid[i], kPhaseLists);
       }
     }
     const bool listed = active && !odd && !lost;
@@ -643,8 +650,8 @@ __global__ void __launch_bounds__(kListWarps * 32) k_build_lists(Dev d) {
   // warp max of the counts -> capacity check
   maxcnt = warp_max(maxcnt);
   if (lane == 0 && maxcnt > 0) {
-    atomicMax(&d.err_info[1], maxcnt);
-    if (maxcnt > cap) atomicOr(d.status, (unsigned)kStatCapacity);
+    atomicMax(&d.err_info[kErrMaxCount], maxcnt);
+    if (maxcnt > cap) raise_status(d, kStatCapacity, 0, kPhaseLists);
   }
 }
 
@@ -654,6 +661,7 @@ __global__ void __launch_bounds__(kListWarps * 32) k_build_lists(Dev d) {
 __global__ void k_colloid_cells(Dev d, int nboxes) {
   const int b = blockIdx.x;
   if (b >= nboxes) return;
+  if (step_aborted(d)) return;
   const BoxParams& p = d.box[b];
   const int n = p.N_colloids;
   if (n < 2) return;
@@ -698,6 +706,7 @@ __global__ void k_density(Dev d) {
   using V = typename V4<T>::type;
   const int i = blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= d.Ntot) return;
+  if (step_aborted(d)) return;
   // positions: the double state itself, or its float copy in mixed precision
   const V* __restrict__ P = sizeof(T) == 8 ? reinterpret_cast<const V*>(d.pos)
                                            : reinterpret_cast<const V*>(d.pos_f);
@@ -754,6 +763,7 @@ __global__ void __launch_bounds__(kDensWarps * 32) k_density_cells(Dev d) {
   const int w = threadIdx.x >> 5, lane = threadIdx.x & 31;
   const int cell = blockIdx.x * kDensWarps + w;
   if (cell >= d.Ctot) return;  // whole warps only
+  if (step_aborted_warp(d)) return;
   const V* __restrict__ P = sizeof(T) == 8 ? reinterpret_cast<const V*>(d.pos)
                                            : reinterpret_cast<const V*>(d.pos_f);
   const int b = d.cell_box[cell];
@@ -871,6 +881,7 @@ template <typename T>
 __global__ void k_pressure(Dev d) {
   const int i = blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= d.Ntot) return;
+  if (step_aborted(d)) return;
   const int ti = d.tinfo[i];
   const BoxParams& p = d.box[box_of(ti)];
   const double dens = d.dens[i];
@@ -1109,6 +1120,7 @@ __global__ void __launch_bounds__(PairShape<T, DIM>::kWarps * 32, PairShape<T, D
   const int w = threadIdx.x >> 5, lane = threadIdx.x & 31;
   const int wbase = (blockIdx.x * Sh::kWarps + w) * 32;
   if (wbase >= d.Ntot) return;  // whole warps only: the lanes below cooperate
+  if (step_aborted_warp(d)) return;
   const int i = wbase + lane;
   const bool active = i < d.Ntot;
   const int is = active ? i : wbase;  // lanes past the end mirror a valid slot, compute nothing
@@ -1140,6 +1152,7 @@ __global__ void __launch_bounds__(PairShape<T, DIM>::kWarps * 32, PairShape<T, D
 __global__ void k_ext_force(Dev d) {
   const int i = blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= d.Ntot) return;
+  if (step_aborted(d)) return;
   const int ti = d.tinfo[i];
   if (type_of(ti) != 0) return;
   const BoxParams& p = d.box[box_of(ti)];
@@ -1166,6 +1179,7 @@ __global__ void k_ext_force(Dev d) {
 __global__ void k_dcdt(Dev d) {
   const int i = blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= d.Ntot) return;
+  if (step_aborted(d)) return;
   const int ti = d.tinfo[i];
   const int Np = d.Npad;
   if (type_of(ti) != 0) {
@@ -1236,6 +1250,7 @@ __global__ void __launch_bounds__(kRedThreads) k_wall_forces(Dev d) {
   __shared__ double sh[3][kRedThreads];
   const int k = blockIdx.x;
   if (k >= d.nwallchunks) return;
+  if (step_aborted(d)) return;
   const int j0 = d.wall_chunk[k], j1 = d.wall_chunk[k + 1];
   const int Np = d.Npad;
   double v[3] = {0.0, 0.0, 0.0};
@@ -1258,6 +1273,7 @@ __global__ void k_wall_forces_final(Dev d) {
   const int w = blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5);
   const int lane = threadIdx.x & 31;
   if (w >= d.nwallseg) return;
+  if (step_aborted(d)) return;
   const int c0 = d.wall_seg_chunk[w], c1 = d.wall_seg_chunk[w + 1];
   double v[3] = {0.0, 0.0, 0.0};
   for (int c = c0 + lane; c < c1; c += 32) {
@@ -1280,6 +1296,7 @@ __global__ void __launch_bounds__(kRedThreads) k_collect_colloids(Dev d) {
   __shared__ double sh[6][kRedThreads];
   const int c = blockIdx.x;
   if (c >= d.ncoll) return;
+  if (step_aborted(d)) return;
   const BoxParams& p = d.box[d.coll_box[c]];
   const int nc = d.ncoll, Np = d.Npad;
   const double cx = d.cs[CS_X * nc + c], cy = d.cs[CS_Y * nc + c], cz = d.cs[CS_Z * nc + c];
@@ -1364,6 +1381,7 @@ __device__ __forceinline__ int coll_neigh_cells(const BoxParams& p, double x, do
 __global__ void k_colloid_pairs(Dev d) {
   const int c = blockIdx.x * blockDim.x + threadIdx.x;
   if (c >= d.ncoll) return;
+  if (step_aborted(d)) return;
   const int b = d.coll_box[c];
   const BoxParams& p = d.box[b];
   if (p.N_colloids < 2) return;
@@ -1425,6 +1443,7 @@ __global__ void k_colloid_pairs(Dev d) {
 // it; mode 1: current step.
 __global__ void k_advance_time(Dev d, int nboxes, int mode) {
   const int b = blockIdx.x * blockDim.x + threadIdx.x;
+  if (step_aborted(d)) return;
   const long long step = *d.step + (mode == 0 ? 1 : 0);
   if (b < nboxes) {
     const BoxParams& p = d.box[b];
@@ -1436,6 +1455,7 @@ __global__ void k_advance_time(Dev d, int nboxes, int mode) {
 }
 
 __global__ void k_count_step(Dev d) {
+  if (step_aborted(d)) return;
   if (threadIdx.x == 0 && blockIdx.x == 0) *d.step += 1;
 }
 

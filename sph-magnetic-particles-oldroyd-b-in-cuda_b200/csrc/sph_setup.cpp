@@ -12,7 +12,10 @@
 #include <string>
 #include <vector>
 
+#include <algorithm>
+#include <cerrno>
 #include <climits>
+#include <thread>
 
 #include "sph_internal.h"
 
@@ -351,25 +354,103 @@ sph_status colloid_shells(HostBox* hb, const double dx[3], int Nmax, std::string
   return SPH_OK;
 }
 
+inline bool is_space(char c) {
+  return c == ' ' || c == '\n' || c == '\t' || c == '\r' || c == '\v' || c == '\f';
+}
+
+// The numbers of a text file read one after another as float, as a sequence of formatted
+// float reads does, parsed in parallel chunks split at whitespace.  A token is a number only
+// if it is made of digits, signs, '.', 'e' and 'E' and converts in full without overflow;
+// reading stops at the first token that is not (as a formatted read fails there).  The
+// conversion is strtof's, the correctly rounded one a formatted float read also uses.
+bool read_float_tokens(const char* path, std::vector<float>* out) {
+  FILE* f = std::fopen(path, "rb");
+  if (!f) return false;
+  std::string buf;
+  char tmp[1 << 16];
+  size_t got;
+  while ((got = std::fread(tmp, 1, sizeof(tmp), f)) > 0) buf.append(tmp, got);
+  std::fclose(f);
+  const size_t n = buf.size();
+  unsigned hw = std::thread::hardware_concurrency();
+  const int nt = (int)std::max<size_t>(1, std::min<size_t>(hw ? hw : 1, n / (1 << 20) + 1));
+  std::vector<size_t> cut(nt + 1, n);
+  cut[0] = 0;
+  for (int t = 1; t < nt; ++t) {
+    size_t c = std::max(cut[t - 1], n * t / nt);
+    while (c < n && !is_space(buf[c])) ++c;
+    cut[t] = c;
+  }
+  std::vector<std::vector<float>> part(nt);
+  std::vector<char> stopped(nt, 0);
+  auto work = [&](int t) {
+    const char* p = buf.data() + cut[t];
+    const char* e = buf.data() + cut[t + 1];
+    std::vector<float>& v = part[t];
+    v.reserve((size_t)(e - p) / 10);
+    while (p < e) {
+      while (p < e && is_space(*p)) ++p;
+      if (p >= e) break;
+      const char* q = p;
+      bool chars_ok = true;
+      while (q < e && !is_space(*q)) {
+        const char c = *q;
+        chars_ok = chars_ok && ((c >= '0' && c <= '9') || c == '+' || c == '-' || c == '.' ||
+                                c == 'e' || c == 'E');
+        ++q;
+      }
+      if (!chars_ok || q - p > 64) {
+        stopped[t] = 1;
+        return;
+      }
+      char tok[72];
+      std::memcpy(tok, p, (size_t)(q - p));
+      tok[q - p] = 0;
+      char* end = nullptr;
+      errno = 0;
+      const float x = std::strtof(tok, &end);
+      if (end != tok + (q - p) || (errno == ERANGE && std::fabs(x) > 1.0f)) {
+        stopped[t] = 1;
+        return;
+      }
+      v.push_back(x);
+      p = q;
+    }
+  };
+  std::vector<std::thread> th;
+  for (int t = 1; t < nt; ++t) th.emplace_back(work, t);
+  work(0);
+  for (auto& x : th) x.join();
+  out->clear();
+  for (int t = 0; t < nt; ++t) {
+    out->insert(out->end(), part[t].begin(), part[t].end());
+    if (stopped[t]) break;
+  }
+  return true;
+}
+
 // Restart file (system_initialize_particles_old_sim.cpp:17-112); values go through float.
+// Rows are taken while a whole row of numbers can be read.
 sph_status restart_particles(HostBox* hb, const char* path, std::string* msg) {
-  std::ifstream f(path ? path : "input_particles.in");
-  if (!f.is_open()) {
+  std::vector<float> tok;
+  if (!read_float_tokens(path ? path : "input_particles.in", &tok)) {
     *msg = "cannot open restart particle file";
     return SPH_ERR_IO;
   }
   const int dim = hb->p.dim;
   const int ncol = dim == 2 ? 9 : 14;
-  std::vector<float> row(ncol);
   auto clear = [](std::vector<double>& v) { v.clear(); };
   for (auto* v : {&hb->x, &hb->y, &hb->z, &hb->vx, &hb->vy, &hb->vz, &hb->mass, &hb->cxx,
                   &hb->cxy, &hb->cyy, &hb->cxz, &hb->cyz, &hb->czz})
     clear(*v);
   hb->type.clear();
-  for (;;) {
-    bool ok = true;
-    for (int k = 0; k < ncol && ok; ++k) ok = static_cast<bool>(f >> row[k]);
-    if (!ok) break;
+  const size_t nrows = tok.size() / (size_t)ncol;
+  for (auto* v : {&hb->x, &hb->y, &hb->z, &hb->vx, &hb->vy, &hb->vz, &hb->mass, &hb->cxx,
+                  &hb->cxy, &hb->cyy, &hb->cxz, &hb->cyz, &hb->czz})
+    v->reserve(nrows);
+  hb->type.reserve(nrows);
+  for (size_t r = 0; r < nrows; ++r) {
+    const float* row = tok.data() + r * ncol;
     if (dim == 2) {
       hb->x.push_back(row[0]); hb->y.push_back(row[1]); hb->z.push_back(0.0);
       hb->vx.push_back(row[2]); hb->vy.push_back(row[3]); hb->vz.push_back(0.0);

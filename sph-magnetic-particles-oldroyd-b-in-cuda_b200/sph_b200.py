@@ -52,7 +52,8 @@ EXPORTS = [
     "sph_kinetic_energy", "sph_last_step_ms", "sph_kernel_launches", "sph_host_setup",
     "sph_profile_phases", "sph_phase_name", "sph_save_checkpoint", "sph_load_checkpoint",
     "sph_observe", "sph_observables", "sph_reset_observables", "sph_get_tuning",
-    "sph_set_tuning", "sph_autotune",
+    "sph_set_tuning", "sph_autotune", "sph_neighbours_search_noalloc", "sph_neighbour_lists",
+    "sph_write_restart",
 ]
 OBSERVABLES = ["wall_stress", "N1", "chain_order", "kinetic_energy"]
 
@@ -232,6 +233,53 @@ def host_setup(input_path, particles_path=None):
     return arrays, res
 
 
+def write_restart(path, dim, a):
+    """Write `a` (the arrays host_setup returns: x, y, z, vx, vy, vz, mass, type, cxx ... czz)
+    as the reference's restart file input_particles.in (include/sph_io.h: sph_write_restart),
+    every value rounded to float as the reference reads it.  Formatted on all host cores."""
+    L = lib()
+    L.sph_write_restart.argtypes = [c_char_p, c_int, c_int] + [PD] * 7 + [PI] + [PD] * 6
+    n = len(a["x"])
+    d = {k: np.ascontiguousarray(a[k], dtype=np.float64)
+         for k in ["x", "y", "z", "vx", "vy", "vz", "mass", "cxx", "cxy", "cyy", "cxz", "cyz", "czz"]}
+    t = np.ascontiguousarray(a["type"], dtype=np.int32)
+    P = lambda k: d[k].ctypes.data_as(PD)
+    st = L.sph_write_restart(str(path).encode(), int(dim), n, P("x"), P("y"), P("z"), P("vx"),
+                             P("vy"), P("vz"), P("mass"), t.ctypes.data_as(PI), P("cxx"),
+                             P("cxy"), P("cyy"), P("cxz"), P("cyz"), P("czz"))
+    if st != 0:
+        raise SphError(st, "sph_write_restart failed for %s" % path)
+
+
+def write_seeded_start(workdir, spec, seed, vmax):
+    """A lattice box started from seeded random fluid velocities, the way the reference can
+    take one: new_sim = 1 with a restart file (src/system_initialize_particles_old_sim.cpp).
+    Positions, masses, types and c = I are the lattice state the reference builds for
+    new_sim = 0 (the engine's host set-up, no GPU needed); every fluid velocity component is
+    drawn uniform in [-vmax, vmax] from `seed`; walls and colloid particles stay at rest, as
+    the lattice start has them.  Writes `workdir`/input (new_sim = 1) and
+    `workdir`/input_particles.in; returns (input path, particles path, N)."""
+    import sph_input
+
+    spec = dict(spec)
+    spec.pop("new_sim", None)
+    lattice_in = os.path.join(workdir, "input_lattice")
+    sph_input.write_input(lattice_in, **spec)
+    a, info = host_setup(lattice_in)
+    n = len(a["x"])
+    rng = np.random.default_rng(seed)
+    v = rng.uniform(-vmax, vmax, size=(3, n))
+    v[:, a["type"] != 0] = 0.0
+    if info["dim"] == 2:
+        v[2] = 0.0
+    a = dict(a, vx=v[0], vy=v[1], vz=v[2])
+    pp = os.path.join(workdir, "input_particles.in")
+    write_restart(pp, info["dim"], a)
+    inp = os.path.join(workdir, "input")
+    sph_input.write_input(inp, new_sim=1, **spec)
+    return inp, pp, n
+
+
 class SphGrid(ctypes.Structure):
     _fields_ = [("dim", c_int), ("wall", c_int), ("Ncells", c_int * 3),
                 ("cell_size", c_double * 3), ("wall_width", c_double)]
@@ -361,6 +409,15 @@ class System:
         v = c_double()
         self._ok(lib().sph_last_step_ms(self._h, ctypes.byref(v)))
         return v.value
+
+    def neighbour_lists(self):
+        """{'capacity', 'max_used', 'grown'}: list row capacity, the largest row needed so
+        far, and how many times the lists have grown."""
+        cap, used, grown = c_int(0), c_int(0), c_int(0)
+        lib().sph_neighbour_lists.argtypes = [c_void_p, PI, PI, PI]
+        self._ok(lib().sph_neighbour_lists(self._h, ctypes.byref(cap), ctypes.byref(used),
+                                           ctypes.byref(grown)))
+        return {"capacity": cap.value, "max_used": used.value, "grown": grown.value}
 
     def kernel_launches(self):
         v = ctypes.c_longlong()

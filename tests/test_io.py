@@ -170,3 +170,64 @@ def test_writer_rejects_bad_arguments(lib, tmp_path):
     assert lib.sph_write_walls(p, 4, 1, P(z), P(z), P(z)) != 0
     assert lib.sph_write_walls(str(tmp_path / "no" / "dir.dat").encode(), 2, 1, P(z), P(z),
                                P(z)) == 9  # SPH_ERR_IO
+
+
+@pytest.mark.parametrize("dim,n", [(2, 900), (3, 40000)])
+def test_restart_file_writer(tmp_path, dim, n):
+    """sph_write_restart writes the same bytes as the reference-format writer in
+    sph_input.write_particles (every value rounded to float, "%.9g"), and the engine's own
+    restart reader (host set-up, no GPU) reads back exactly those floats."""
+    import sph_input
+
+    rng = np.random.default_rng(dim * 7 + n)
+    a = {k: rng.normal(0, 10.0 ** rng.integers(-7, 3), n)
+         for k in ["x", "y", "z", "vx", "vy", "vz", "mass", "cxx", "cxy", "cyy", "cxz", "cyz",
+                   "czz"]}
+    a["x"] = rng.uniform(0.0, 1.0, n)
+    a["y"] = rng.uniform(0.0, 1.0, n)
+    a["z"] = rng.uniform(0.0, 1.0, n) if dim == 3 else np.zeros(n)
+    a["mass"] = np.full(n, 1.0 / n)
+    a["type"] = np.zeros(n, dtype=np.int32)
+    a["vx"][:4] = [-0.0, 1e-45, 3.4e38, 0.1]
+    p_c = str(tmp_path / "c.in")
+    p_py = str(tmp_path / "py.in")
+    sph_b200.write_restart(p_c, dim, a)
+    sph_input.write_particles(p_py, dim, a["x"], a["y"], a["z"], a["vx"], a["vy"], a["vz"],
+                              a["mass"], a["type"], a["cxx"], a["cxy"], a["cyy"], a["cxz"],
+                              a["cyz"], a["czz"])
+    assert open(p_c).read() == open(p_py).read()
+    side = int(round(n ** (1.0 / dim)))
+    inp = str(tmp_path / "input")
+    sph_input.write_input(inp, N=(side,) * dim, L=(1.0,) * dim, dim=dim, overlap=3.0, new_sim=1)
+    got, info = sph_b200.host_setup(inp, p_c)
+    assert info["N"] == n
+    f32 = lambda v: np.asarray(v, dtype=np.float32).astype(np.float64)
+    for k in ["x", "y", "vx", "vy", "cxy"] + (["z", "vz", "czz"] if dim == 3 else []):
+        assert np.array_equal(got[k], f32(a[k])), k
+
+
+def test_seeded_start(tmp_path):
+    """write_seeded_start: the lattice of new_sim = 0 with seeded fluid velocities in
+    [-vmax, vmax], walls at rest, every value rounded to float as the reference reads it."""
+    import sph_input
+
+    spec = dict(N=(12, 12, 12), L=(1.0, 1.0, 1.0), dim=3, overlap=3.0, wall=1,
+                Vwall_bottom=-0.5, Vwall_top=0.5, dt=2e-5)
+    inp, pp, n = sph_b200.write_seeded_start(str(tmp_path), spec, seed=3, vmax=0.01)
+    lattice, _ = sph_b200.host_setup(str(tmp_path / "input_lattice"))
+    got, info = sph_b200.host_setup(inp, pp)
+    assert info["N"] == n == len(lattice["x"])
+    f32 = lambda v: np.asarray(v, dtype=np.float32).astype(np.float64)
+    for k in ["x", "y", "z", "mass", "cxx", "cyy"]:
+        assert np.array_equal(got[k], f32(lattice[k])), k
+    assert np.array_equal(got["type"], lattice["type"])
+    fluid = got["type"] == 0
+    for k in ["vx", "vy", "vz"]:
+        v = got[k]
+        assert np.all(np.abs(v[fluid]) <= 0.01) and np.all(v[~fluid] == 0.0)
+        assert np.std(v[fluid]) > 0.004
+    other = tmp_path / "again"
+    other.mkdir()
+    sph_b200.write_seeded_start(str(other), spec, seed=3, vmax=0.01)
+    assert open(pp).read() == open(str(other / "input_particles.in")).read()
+    assert "new_sim 1" in open(inp).read() and sph_input.DEFAULTS["new_sim"] == 0
