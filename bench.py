@@ -175,15 +175,43 @@ def write_workload(d, lattice=128):
 
 
 def particles_file(input_path):
-    return os.path.join(os.path.dirname(input_path), "input_particles.in")
+    """The restart file beside an input, or None when the input starts from the lattice."""
+    p = os.path.join(os.path.dirname(input_path), "input_particles.in")
+    return p if os.path.exists(p) else None
 
 
-def cpu_baseline(workdir, steps=1):
+SUSPENSION_NAME = ("suspension3d_96: 96^3 Oldroyd-B fluid between walls at rest with 32 rotating "
+                   "magnetic colloids of radius 4 dx (sph_input.suspension_spec, seed 11)")
+SUSPENSION_METRIC = "particle-steps/s (96^3 magnetic suspension, 32 colloids)"
+
+
+def write_suspension(d, lattice=96):
+    """The 3D magnetic suspension input in directory d (lattice start, no restart file)."""
+    path = os.path.join(d, "input")
+    sph_input.write_input(path, **sph_input.suspension_spec(N=lattice))
+    return path
+
+
+class Workload:
+    """A single-box benchmark workload: its name, metric and input writer."""
+
+    def __init__(self, key, name, metric, write, lattice):
+        self.key, self.name, self.metric, self.write, self.lattice = key, name, metric, write, lattice
+
+
+WORKLOADS = {
+    "couette3d": Workload("couette3d", WORKLOAD_NAME, METRIC, write_workload, 128),
+    "suspension96": Workload("suspension96", SUSPENSION_NAME, SUSPENSION_METRIC, write_suspension,
+                             96),
+}
+
+
+def cpu_baseline(workdir, wl, steps=1):
     """The FP64 OpenMP oracle on this host: initial forces, then `steps` timed steps."""
     import oracle
 
     cores = oracle.set_threads(os.cpu_count() or 1)
-    inp = write_workload(workdir)
+    inp = wl.write(workdir)
     o = oracle.Oracle(inp, particles_file(inp))
     o.run(0)
     t0 = time.perf_counter()
@@ -192,8 +220,8 @@ def cpu_baseline(workdir, steps=1):
     n = o.info()["N"]
     o.close()
     return {"value": n * steps / dt, "unit": UNIT, "cores": cores, "kind": "port",
-            "sample": "CPU oracle (C99+OpenMP FP64 restatement) on the full 128^3 workload: "
-                      "initial forces untimed, then %d timed step(s), %.1f s" % (steps, dt)}
+            "sample": "CPU oracle (C99+OpenMP FP64 restatement) on the full %s workload: "
+                      "initial forces untimed, then %d timed step(s), %.1f s" % (wl.key, steps, dt)}
 
 
 def dist_setup(args):
@@ -222,23 +250,31 @@ def max_over_ranks(dist, value, local):
     return float(t.item())
 
 
-def run_reference(args, world, rank, dist):
+def run_reference(args, world, rank, dist, wl):
     """The reference's own CUDA build (oracle/_ref/ref_sph: its unmodified sources driven by
     oracle/ref_harness.cu), timed with CUDA events around the step loop."""
     if rank != 0:
         return 0
-    ref = os.path.join(ROOT, "oracle", "_ref", "ref_sph")
-    line = {"impl": "reference", "metric": METRIC, "unit": UNIT, "n_gpus": 1, "steps": args.steps,
-            "warmup": args.warmup, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
-            "dtype": "f64", "data": "synthetic",
-            "config": {"workload": WORKLOAD_NAME, "implementation": "reference CUDA build, FP64, "
-                                                                  "sm_100a, as shipped"}}
+    # FP64: the reference as shipped; with --precision mixed, its FP32 configuration
+    # (real = float in src/config.h), the same-precision baseline of the mixed engine
+    fp32 = args.precision != "fp64"
+    rel = os.path.join("oracle", "_ref", "fp32", "ref_sph") if fp32 else \
+        os.path.join("oracle", "_ref", "ref_sph")
+    ref = os.path.join(ROOT, rel)
+    impl = ("reference CUDA build, real = float (its src/config.h FP32 switch), sm_100a"
+            if fp32 else "reference CUDA build, FP64, sm_100a, as shipped")
+    line = {"impl": "reference", "metric": wl.metric, "unit": UNIT, "n_gpus": 1,
+            "steps": args.steps, "warmup": args.warmup, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f32" if fp32 else "f64",
+            "data": "synthetic",
+            "config": {"workload": wl.name, "precision": args.precision,
+                       "implementation": impl}}
     if not os.path.exists(ref):
-        line["unavailable"] = "reference build oracle/_ref/ref_sph is missing (build() compiles it)"
+        line["unavailable"] = "reference build %s is missing (build() compiles it)" % rel
         print(json.dumps(line))
         return 0
     with tempfile.TemporaryDirectory() as wd:
-        write_workload(wd)
+        wl.write(wd)
         with ClockSampler(int(os.environ.get("LOCAL_RANK", "0"))) as clk:
             r = subprocess.run([ref, "time", str(args.steps), str(args.warmup)], cwd=wd,
                                capture_output=True, text=True, timeout=3600)
@@ -264,12 +300,13 @@ def run_reference(args, world, rank, dist):
     return 0
 
 
-def run_ours(args, world, rank, local, dist):
+def run_ours(args, world, rank, local, dist, wl):
     import sph_b200
 
     with tempfile.TemporaryDirectory() as wd:
-        path = write_workload(wd, args.lattice)
-        sysm = sph_b200.System(path, [particles_file(path)], precision=args.precision,
+        path = wl.write(wd, args.lattice)
+        pp = particles_file(path)
+        sysm = sph_b200.System(path, [pp] if pp else None, precision=args.precision,
                                device=local)
         n = sysm.N
         tuning = sysm.autotune() if not args.no_autotune else sysm.tuning()
@@ -315,12 +352,14 @@ def run_ours(args, world, rank, local, dist):
     achieved = B_ALG_PAIRS[args.precision] * n / (pair_ms * 1e-3) / 1e9
     step_gbs = B_ALG_STEP[args.precision] * n * args.steps / (ms * 1e-3) / 1e9
     line = {
-        "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
+        "metric": wl.metric, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
         "warmup": args.warmup, "ms_per_step": ms_max / args.steps, "higher_is_better": True,
         "scaling": "weak", "vs_baseline": None,
         "dtype": "f64" if args.precision == "fp64" else "f32 pairs / f64 state",
-        "data": "synthetic (lattice, fluid velocities seeded uniform in +-1e-3 c, seed %d)" % SEED,
-        "config": {"workload": WORKLOAD_NAME, "particles": n, "precision": args.precision,
+        "data": ("synthetic (lattice, fluid velocities seeded uniform in +-1e-3 c, seed %d)" % SEED
+                 if wl.key == "couette3d" else
+                 "synthetic (lattice at rest, seeded colloid centres)"),
+        "config": {"workload": wl.name, "particles": n, "precision": args.precision,
                    "parallelism": "replicas only" if world > 1 else "single box",
                    "launch_geometry": tuning,
                    "l2": "inputs larger than L2 (state ~0.7 GB > 126 MB), no flush",
@@ -333,7 +372,7 @@ def run_ours(args, world, rank, local, dist):
                              "fraction is reported as the metric asks"},
         "hbm_frac_step": step_gbs / hbm,
         "phase_ms": phases,
-        "roofline_fp64": None if args.precision != "fp64" else {
+        "roofline_fp64": None if (args.precision != "fp64" or wl.key != "couette3d") else {
             "kernel": "k_pairs", "bound": "fp64",
             "achieved": FP64_PAIR_FLOP * n / (pair_ms * 1e-3) / 1e12,
             "peak": FP64_LANES * 2 * clock_mhz() * 1e6 / 1e12, "unit": "TFLOP/s",
@@ -347,9 +386,76 @@ def run_ours(args, world, rank, local, dist):
     }
     if world == 1 and not args.no_cpu_baseline:
         with tempfile.TemporaryDirectory() as wd:
-            line["cpu_baseline"] = cpu_baseline(wd, steps=1)
+            line["cpu_baseline"] = cpu_baseline(wd, wl, steps=1)
+    if world == 1 and not args.no_secondary and wl.key == "couette3d" and args.lattice == 128:
+        line["secondary"] = secondary_figures(args, local, wl)
     print(json.dumps(line))
     return 0
+
+
+def mixed_summary(args, local, wl, steps=10, cmp_steps=5):
+    """The same workload in mixed precision (pair sums in float with compensated
+    accumulation, state in FP64): device time per step, and its deviation from the FP64
+    engine after cmp_steps steps from the same start (max |mixed - fp64| / group scale)."""
+    import sph_b200
+
+    # field groups: positions and c on their natural scale 1, the rest on the group's largest
+    # FP64 magnitude
+    groups = {"pos": (["x", "y", "z"], 1.0), "vel": (["vx", "vy", "vz"], None),
+              "dens": (["dens"], None), "force": (["fx", "fy", "fz"], None),
+              "conf": (["cxx", "cxy", "cyy", "cxz", "cyz", "czz"], 1.0),
+              "dcdt": (["dcdt_xx", "dcdt_xy", "dcdt_yy", "dcdt_xz", "dcdt_yz", "dcdt_zz"], None)}
+
+    def group_error(get_a, get_b, fields, scale):
+        a = np.concatenate([get_a(f) for f in fields])
+        b = np.concatenate([get_b(f) for f in fields])
+        sc = scale if scale else max(float(np.abs(b).max()), 1e-300)
+        return float(np.abs(a - b).max() / sc)
+
+    with tempfile.TemporaryDirectory() as wd:
+        path = wl.write(wd, args.lattice)
+        pp = particles_file(path)
+        b = sph_b200.System(path, [pp] if pp else None, precision="mixed", device=local)
+        a = sph_b200.System(path, [pp] if pp else None, precision="fp64", device=local)
+        a.step(cmp_steps)
+        b.step(cmp_steps)
+        a.synchronize()
+        b.synchronize()
+        errs = {g: group_error(b.field, a.field, f, sc) for g, (f, sc) in groups.items()}
+        wa, wb = a.wall_forces(), b.wall_forces()
+        errs["walls"] = float(np.abs(wa - wb).max() / np.abs(wa).max())
+        a.close()
+        b.step(3)
+        b.synchronize()
+        b.step(steps)
+        b.synchronize()
+        ms = b.last_step_ms() / steps
+        n = b.N
+        b.close()
+    return {"precision": "mixed", "ms_per_step": ms, "value": n / (ms * 1e-3), "unit": UNIT,
+            "steps": steps, "error_vs_fp64_after_%d_steps" % cmp_steps: errs,
+            "timing": "CUDA events around sph_step(%d) after 3 warm-up steps" % steps}
+
+
+def secondary_figures(args, local, wl):
+    """Short measurements of the other workloads, recorded beside the headline: the mixed-
+    precision engine on this workload, the 512-box batched ensemble against the same boxes
+    run one at a time, and the surrogate's training throughput."""
+    out = {}
+    t0 = time.perf_counter()
+    out["mixed_precision_128"] = mixed_summary(args, local, wl)
+    sub = argparse.Namespace(**vars(args))
+    sub.steps, sub.warmup, sub.e2e_steps, sub.precision = 10, 3, 3, "fp64"
+    ens = run_ensemble(sub, 1, 0, local, None, emit=False)
+    out["ensemble512_fp64"] = {k: ens[k] for k in ("value", "unit", "ms_per_step", "steps",
+                                                    "looped_single_box", "batched_over_looped")
+                               if k in ens}
+    sub.steps, sub.warmup = 200, 20
+    sur = run_surrogate_train(sub, 1, 0, local, None, emit=False)
+    out["surrogate_training"] = {k: sur[k] for k in ("metric", "value", "unit", "ms_per_step",
+                                                      "steps", "roofline") if k in sur}
+    out["seconds"] = time.perf_counter() - t0
+    return out
 
 
 ENSEMBLE_NAME = ("ensemble512: 512 independent 2D wall-bounded Oldroyd-B boxes with rotating "
@@ -368,7 +474,7 @@ def timed_single_box(sph_b200, path, precision, device, steps, warmup=3):
     return ms, n
 
 
-def run_ensemble(args, world, rank, local, dist):
+def run_ensemble(args, world, rank, local, dist, emit=True):
     """The batched workload: 512 boxes advanced together in one context per GPU (boxes
     sharded over ranks by particle-steps, no exchange during the run), against the same
     boxes run one at a time."""
@@ -446,8 +552,10 @@ def run_ensemble(args, world, rank, local, dist):
     if looped:
         line["looped_single_box"] = looped
         line["batched_over_looped"] = value / looped["value"]
-    print(json.dumps(line))
-    return 0
+    if emit:
+        print(json.dumps(line))
+        return 0
+    return line
 
 
 SWEEP_NAME = ("sweep: 2D wall-bounded Oldroyd-B boxes with magnetic colloids at side 64, six "
@@ -541,7 +649,7 @@ def run_sweep_bench(args, world, rank, local, dist):
     return 0
 
 
-def run_surrogate_train(args, world, rank, local, dist):
+def run_surrogate_train(args, world, rank, local, dist, emit=True):
     """Training throughput of the surrogate network (5 heads, batch 1024) on its tensor-core
     kernels: samples per second and the dense FLOP rate of the training step."""
     import torch
@@ -588,8 +696,10 @@ def run_surrogate_train(args, world, rank, local, dist):
                                  "tensor work and is launch- and latency-bound"},
             "clocks": clk.summary()}
     net.close()
-    print(json.dumps(line))
-    return 0
+    if emit:
+        print(json.dumps(line))
+        return 0
+    return line
 
 
 def main():
@@ -599,10 +709,11 @@ def main():
     ap.add_argument("--sweep-train", type=int, default=20480)
     ap.add_argument("--sweep-train-steps", type=int, default=3000)
     ap.add_argument("--workload", default="couette3d",
-                    choices=["couette3d", "ensemble512", "sweep", "surrogate"],
-                    help="couette3d: the headline 128^3 box; ensemble512: 512 batched boxes; "
-                         "sweep: sweep points per hour with the surrogate; surrogate: the "
-                         "network's training throughput")
+                    choices=["couette3d", "suspension96", "ensemble512", "sweep", "surrogate"],
+                    help="couette3d: the headline 128^3 box; suspension96: the 96^3 box with 32 "
+                         "magnetic colloids; ensemble512: 512 batched boxes; sweep: sweep "
+                         "points per hour with the surrogate; surrogate: the network's "
+                         "training throughput")
     ap.add_argument("--steps", type=int, default=50)
     ap.add_argument("--warmup", type=int, default=5)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
@@ -614,21 +725,30 @@ def main():
                     help="ncu DRAM bytes per k_pairs launch (default: the FP64 capture at "
                          "96^3, 786.6 MB, scaled by particle count to the benchmark)")
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-secondary", action="store_true",
+                    help="skip the short mixed-precision, ensemble and surrogate figures that "
+                         "the default couette3d line carries under 'secondary'")
     ap.add_argument("--no-autotune", action="store_true",
                     help="keep the default launch geometry (profiling runs: no tuning launches)")
-    ap.add_argument("--lattice", type=int, default=128,
-                    help="lattice side; 128 is the benchmark, smaller sizes only for ncu captures")
+    ap.add_argument("--lattice", type=int, default=None,
+                    help="lattice side; the workload's own (128 for couette3d, 96 for "
+                         "suspension96) is the benchmark, smaller sizes only for ncu captures")
     args = ap.parse_args()
-    if args.pairs_traffic is None and args.lattice == 128 and args.precision in (None, "fp64"):
+    wl = WORKLOADS.get(args.workload)
+    if wl is not None:
+        if args.lattice is None:
+            args.lattice = wl.lattice
+        if args.lattice != wl.lattice:
+            wl = Workload(wl.key, "%s_%d (profiling size, not the benchmark)" % (wl.key, args.lattice),
+                          wl.metric, wl.write, args.lattice)
+            args.no_cpu_baseline = True
+    if (args.pairs_traffic is None and args.workload == "couette3d" and args.lattice == 128
+            and args.precision in (None, "fp64")):
         # dram__bytes_read.sum + dram__bytes_write.sum of one k_pairs launch at 96^3
         # (940,032 particles), scaled to the 2,195,456 particles of the benchmark
         args.pairs_traffic = (722.4832e6 + 64.10752e6) * 2195456 / 940032
     if args.precision is None:
         args.precision = "mixed" if args.workload == "sweep" else "fp64"
-    if args.lattice != 128:
-        global WORKLOAD_NAME
-        WORKLOAD_NAME = "couette3d_%d (profiling size, not the benchmark)" % args.lattice
-        args.no_cpu_baseline = True
     if args.warmup < 3:
         args.warmup = 3
     world, rank, local, dist = dist_setup(args)
@@ -657,8 +777,8 @@ def main():
                 return 0
             return run_ensemble(args, world, rank, local, dist)
         if args.impl == "reference":
-            return run_reference(args, world, rank, dist)
-        return run_ours(args, world, rank, local, dist)
+            return run_reference(args, world, rank, dist, wl)
+        return run_ours(args, world, rank, local, dist, wl)
     finally:
         if dist is not None:
             dist.destroy_process_group()

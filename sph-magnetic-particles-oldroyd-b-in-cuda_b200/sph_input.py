@@ -77,3 +77,60 @@ def write_particles(path, dim, x, y, z, vx, vy, vz, mass, type_, cxx, cxy, cyy,
     # %.9g round-trips every float32 exactly
     np.savetxt(path, data, fmt="%.9g")
     return path
+
+
+def suspension_centres(n, R, rcut, seed, L=(1.0, 1.0, 1.0), min_dist=2.2, tries=100000):
+    """n colloid centres for a 3D box with walls normal to y, drawn uniformly from `seed`:
+    x over the periodic box, y at least R + rcut from both walls, z in [R, L - R]; every
+    pair at least min_dist * R apart (x and z periodic).  Two rules keep the input one the
+    reference accepts: each pair passes its overlap check as it is written,
+    sqrt(dx^2 + dy^2 + dy^2) >= 2R with dx periodic (src/system_read_input.cpp:482-500
+    takes the z difference from the y coordinates); and z stays R clear of the box faces,
+    because the reference places the poles of a colloid's particle shells at z +- r without
+    the periodic wrap (src/system_initialize_particles_new_sim.cpp:196-199,239-242), and a
+    pole below z = 0 hashes outside the cell grid at the first search.  Raises if a centre
+    finds no place in `tries` draws."""
+    rng = np.random.default_rng(seed)
+    lo, hi = R + rcut, L[1] - R - rcut
+    out = []
+    for _ in range(n):
+        for _ in range(tries):
+            c = (rng.uniform(0.0, L[0]), rng.uniform(lo, hi), rng.uniform(R, L[2] - R))
+            ok = True
+            for p in out:
+                dx = c[0] - p[0]
+                dx -= L[0] * round(dx / L[0])
+                dy = c[1] - p[1]
+                dz = c[2] - p[2]
+                dz -= L[2] * round(dz / L[2])
+                if dx * dx + dy * dy + dz * dz < (min_dist * R) ** 2 or \
+                        dx * dx + 2.0 * dy * dy < (2.0 * R) ** 2:
+                    ok = False
+                    break
+            if ok:
+                out.append(c)
+                break
+        else:
+            raise ValueError("no place for colloid %d of %d" % (len(out) + 1, n))
+    return tuple(out)
+
+
+def suspension_spec(N=96, n_colloids=32, seed=11, nsteps=2000, tau_repulsion=1.0):
+    """The 3D suspension of rotating magnetic colloids between walls at rest: N^3 lattice,
+    L = 1, overlap 3, Oldroyd-B (tau 1, np 100, kT 0.01, eta 0.1, rho 1, c 10, P0 0),
+    n_colloids colloids of radius 4 dx (density 1, moving), repulsion cut-on 2.05 R
+    (the reference's cut-on is the surface-to-surface gap, 0.05 R), F0_repulsion 10,
+    magnetic cutoff 6 R, F0_magnetic 5, omega 2 pi, dt 2e-5.  tau_repulsion defaults to 1:
+    the reference rejects 0.01 here (its repulsion cutoff 2R + 5R/tau_rep would exceed the
+    box, src/system_initialize.cpp:161,225-247), and 1 is the smallest round value it
+    accepts."""
+    dx = 1.0 / N
+    R = 4.0 * dx
+    rcut = 3.0 * dx
+    return dict(N=(N, N, N), L=(1.0, 1.0, 1.0), dim=3, overlap=3.0, wall=1, Vwall_bottom=0.0,
+                Vwall_top=0.0, rho=1.0, c=10.0, P0=0.0, eta=0.1, zeta=0.0, np=100.0, kT=0.01,
+                tau=1.0, dt=2e-5, Nsteps=nsteps, N_colloids=n_colloids, coll_R=R,
+                coll_rho=1.0, coll_move=0,
+                coll_x=suspension_centres(n_colloids, R, rcut, seed),
+                coll_repulsion_cuton=0.05 * R, F0_repulsion=10.0, tau_repulsion=tau_repulsion,
+                cutoff_magnetic=6.0 * R, F0_magnetic=5.0, omega_magnetic=2.0 * np.pi)

@@ -108,3 +108,26 @@ def test_reference_z_overlap_quirk(workdir):
         oracle.Oracle(path)
     with pytest.raises(sph_b200.SphError):
         sph_b200.host_setup(path)
+
+
+def test_suspension_spec_is_accepted(tmp_path):
+    """The 96^3 suspension input: 32 seeded colloids the reference's own checks accept
+    (overlap check as written, wall clearance, colloid coarse grid of >= 3 cells), every
+    shell particle inside the cell grid at the first search, reproducible from its seed."""
+    import sph_b200
+    import sph_input
+
+    spec = sph_input.suspension_spec()
+    assert spec == sph_input.suspension_spec() and len(spec["coll_x"]) == 32
+    path = str(tmp_path / "input")
+    sph_input.write_input(path, **spec)
+    a, info = sph_b200.host_setup(path)
+    assert info["N_colloids"] == 32 and min(info["Ncells_colloids"]) >= 3
+    cs, ww, nc = info["cell_size"], info["wall_width"], info["Ncells"]
+    cx = np.floor(a["x"] / cs[0]).astype(int)
+    cy = np.floor((a["y"] + ww) / cs[1]).astype(int)
+    cz = np.floor(a["z"] / cs[2]).astype(int)
+    cx[cx == nc[0]] -= 1
+    cz[cz == nc[2]] -= 1
+    cell = (cz * nc[1] + cy) * nc[0] + cx
+    assert cell.min() >= 0 and cell.max() < info["Ntotal_cells"]
