@@ -35,7 +35,7 @@ def test_oracle_matches_reference_build(name, workdir):
     pp = os.path.join(workdir, "input_particles.in")
     o = oracle.Oracle(os.path.join(workdir, "input"), pp if os.path.exists(pp) else None)
     dim = o.info()["dim"]
-    steps = [0] if name == "colloids3d" else mg.STEPS
+    steps = [0] if name == "colloids3d" else mg.steps_of(name)
     for s in steps:
         o.run(s - o.info()["step"]) if s > 0 else o.run(0)
         keys = {k[len("s%d_" % s):] for k in g.files if k.startswith("s%d_" % s)}

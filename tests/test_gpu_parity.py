@@ -86,9 +86,9 @@ def test_fp64_engine_matches_oracle(name, workdir):
 
 
 LONG = {
-    # config 1 at its own size: 2D Kolmogorov flow, 64^2 = 4,096 particles
-    "kolmogorov64": (dict(N=(64, 64), L=(1.0, 1.0), dim=2, overlap=4.0, ext_force_type=2,
-                          ext_force=(1.0, 0.0), dt=5e-5), 200),
+    # config 1 at its own size and length: 2D Kolmogorov flow, 64^2 = 4,096 particles,
+    # 2000 steps
+    "kolmogorov64": (mg.NEW_CASES["kolmogorov64"], 2000),
     "couette2d": (mg.CASES["couette2d"], 100),
     "colloids2d": (mg.CASES["colloids2d"], 100),
     "colloids3d": (mg.CASES["colloids3d"], 30),
@@ -162,7 +162,7 @@ def test_engine_matches_reference_build(name, workdir):
     g = np.load(os.path.join(HERE, "golden", name + ".npz"))
     e, _ = open_case(name, workdir)
     dim = e.info()["dim"]
-    steps = [0] if name == "colloids3d" else mg.STEPS
+    steps = [0] if name == "colloids3d" else mg.steps_of(name)
     done = 0
     for s in steps:
         e.step(s - done)
