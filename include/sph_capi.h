@@ -81,8 +81,9 @@ typedef struct sph_options {
   int precision;    /* sph_precision                                                   */
   int device;       /* CUDA device ordinal                                             */
   int use_graph;    /* sph_step replays a captured CUDA graph of one step             */
-  int nbr_capacity; /* neighbour slots per particle, rounded up to a multiple of 8;
-                       0 = derived from overlap and dim */
+  int nbr_capacity; /* neighbour-list capacity in candidate chunks per cell (a chunk is
+                       up to 32 consecutive slots of one neighbour cell); 0 = derived
+                       from overlap and dim.  Lists grow when a build needs more. */
   int init_on_device; /* 1: lattice boxes (new_sim 0) are built on the GPU -- sites,
                          colloid carving, wall layers, walls lists -- bit-identical to the
                          host set-up; colloid shells and restart files stay on the host */

@@ -10,6 +10,7 @@
 #include <fstream>
 #include <sstream>
 #include <string>
+#include <type_traits>
 #include <vector>
 
 #include "sph_internal.h"
@@ -125,21 +126,51 @@ void swap_state(sph_ctx* c, bool with_forces) {
   c->parity ^= 1;
 }
 
+// Chunks per row of the neighbour chunk table: every neighbour cell of a cell (3^d of them)
+// gives its particles in chunks of up to 16 (a half warp per cell) or 32 slots.  Sized for
+// cells holding 1.5 times the lattice's particles per cell, in chunks of 16.
 int derived_capacity(const std::vector<HostBox>& boxes, int dim) {
-  double worst = 0;
+  int worst = 1;
   for (const HostBox& hb : boxes) {
     const sph_input& in = hb.in;
-    double vol = 1.0;
-    int Ny = in.N[1];
-    double dx0 = in.L[0] / in.N[0], dx1 = in.L[1] / Ny;
-    vol = dx0 * dx1;
-    if (dim == 3) vol *= in.L[2] / in.N[2];
-    const double rc = hb.p.rcut;
-    double ball = dim == 3 ? 4.0 / 3.0 * M_PI * rc * rc * rc : M_PI * rc * rc;
-    worst = std::max(worst, ball / vol + 1.0);
+    double ppc = 1.0;  // lattice particles per cell
+    for (int q = 0; q < dim; ++q) ppc *= hb.p.cell_size[q] / (in.L[q] / in.N[q]);
+    const int per_cell = (int)std::ceil(1.5 * ppc / 16.0);
+    worst = std::max(worst, (dim == 3 ? 27 : 9) * std::max(per_cell, 1));
   }
-  int cap = (int)std::ceil(1.5 * worst + 32.0);
-  return (cap + 7) / 8 * 8;
+  return worst;
+}
+
+// Own rows of the chunk table for particles listed from their own cells (on the upper box
+// edge): rare, so a small table.
+int derived_odd_rows(int Ntot) { return 256 + Ntot / 1024; }
+
+// Allocates the neighbour-list buffers for `cap` chunks per row and `odd_cap` own rows,
+// replacing any earlier ones.
+bool alloc_lists(sph_ctx* c, int cap, int odd_cap) {
+  Dev& d = c->d;
+  auto replace = [&](auto** ptr, size_t n) {
+    using T = std::remove_pointer_t<std::remove_reference_t<decltype(*ptr)>>;
+    void* q = nullptr;
+    if (cudaMalloc(&q, std::max<size_t>(n, 1) * sizeof(T)) != cudaSuccess) return false;
+    cudaMemsetAsync(q, 0, std::max<size_t>(n, 1) * sizeof(T), c->stream);
+    auto it = std::find(c->allocs.begin(), c->allocs.end(), (void*)*ptr);
+    if (*ptr && it != c->allocs.end()) {
+      cudaFree(*it);
+      *it = q;
+    } else {
+      c->allocs.push_back(q);
+    }
+    *ptr = static_cast<T*>(q);
+    return true;
+  };
+  const size_t rows = (size_t)d.Ctot + odd_cap;
+  if (!replace(&d.nmask, (size_t)cap * d.Npad) || !replace(&d.cbase, rows * cap) ||
+      !replace(&d.cnch, rows))
+    return false;
+  d.cap = cap;
+  d.odd_cap = odd_cap;
+  return true;
 }
 
 // Reads the device error flags and their record (err_info, kErrInfoLen ints) without
@@ -190,19 +221,16 @@ void drop_graphs(sph_ctx* c) {
     }
 }
 
+// Grows the chunk table to hold `needed` chunks per row (with headroom), and its own rows
+// to hold the last list build's count of particles listed from their own cells.
 sph_status grow_capacity(sph_ctx* c, int needed) {
-  int cap = std::max(needed + needed / 4 + 8, c->d.cap + 32);
-  cap = (cap + 7) / 8 * 8;
-  int* nbr = nullptr;
-  if (cudaMalloc(&nbr, (size_t)cap * c->d.Npad * sizeof(int)) != cudaSuccess)
-    return fail(c, SPH_ERR_NOMEM, "cannot grow neighbour lists");
-  auto it = std::find(c->allocs.begin(), c->allocs.end(), (void*)c->d.nbr);
-  if (it != c->allocs.end()) {
-    cudaFree(*it);
-    *it = nbr;
-  }
-  c->d.nbr = nbr;
-  c->d.cap = cap;
+  int odd = 0;
+  if (cudaMemcpy(&odd, c->d.odd_count, sizeof(int), cudaMemcpyDeviceToHost) != cudaSuccess)
+    return cuda_fail(c, "list statistics");
+  const int cap = std::max(needed + needed / 4 + 2, c->d.cap + (needed > c->d.cap ? 4 : 0));
+  const int odd_cap = odd > c->d.odd_cap ? 2 * odd + 64 : c->d.odd_cap;
+  cudaStreamSynchronize(c->stream);
+  if (!alloc_lists(c, cap, odd_cap)) return fail(c, SPH_ERR_NOMEM, "cannot grow neighbour lists");
   c->cap_grown++;
   drop_graphs(c);
   return SPH_OK;
@@ -673,9 +701,7 @@ sph_status sph_create_ensemble(int nboxes, const sph_input* inputs,
   d.ncoll = ncoll;
   d.nwallseg = nwall;
   d.Nlist_coll = nlist;
-  // list rows hold a multiple of 8 entries: rows start 32-byte aligned and are read and
-  // written in aligned 16- and 32-byte groups
-  d.cap = o.nbr_capacity > 0 ? (o.nbr_capacity + 7) / 8 * 8 : derived_capacity(c->boxes, c->dim);
+  const int list_cap = o.nbr_capacity > 0 ? o.nbr_capacity : derived_capacity(c->boxes, c->dim);
   c->key_bits = bits_for(std::max(Ctot, 2));
   const size_t Np = d.Npad;
   bool ok = true;
@@ -700,11 +726,12 @@ sph_status sph_create_ensemble(int nboxes, const sph_input* inputs,
     ok = ok && dalloc(c, &r, Np);
     d.rec = r;
   }
-  ok = ok && dalloc(c, &d.nbr, (size_t)d.cap * Np) && dalloc(c, &d.nbr_cnt, Np);
+  ok = ok && dalloc(c, &d.nbr_cnt, Np) && dalloc(c, &d.crow, Np) && dalloc(c, &d.odd_count, 1);
   ok = ok && dalloc(c, &d.key_by_gid, Np) && dalloc(c, &d.keys, Np) && dalloc(c, &d.vals, Np);
   ok = ok && dalloc(c, &d.keys_alt, Np) && dalloc(c, &d.vals_alt, Np);
   ok = ok && dalloc(c, &d.cell_begin, Ctot + 1) && dalloc(c, &d.cell_start, Ctot);
   ok = ok && dalloc(c, &d.cell_end, Ctot) && dalloc(c, &d.cell_box, Ctot);
+  ok = ok && alloc_lists(c, list_cap, derived_odd_rows(d.Ntot));
   ok = ok && dalloc(c, &d.walls_list, nwl) && dalloc(c, &d.wall_seg, nwall + 1);
   ok = ok && dalloc(c, &d.wall_f, 3 * std::max(nwall, 1));
   d.nwallchunks = nwchunk;

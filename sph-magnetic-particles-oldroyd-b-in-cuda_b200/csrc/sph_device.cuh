@@ -147,6 +147,48 @@ __device__ __forceinline__ void raise_status(const Dev& d, unsigned bit, int inf
   }
 }
 
+// One particle's neighbour candidates in list order, decoded from the hit masks the list
+// build writes: row r = crow[i] of the chunk table holds cnch[r] chunk bases
+// (cbase[r * cap + k]); the particle's mask of chunk k is nmask[k * Npad + i], bit q meaning
+// slot base + q.  Candidates come chunk by chunk and, inside a chunk, by increasing slot,
+// which is the reference's candidate order.  The next chunk's mask and base are loaded one
+// chunk ahead.  next() gives nbr_cnt[i] candidates, then -1.
+struct NbrIter {
+  const unsigned* mcol;  // this particle's masks, stride np
+  const int* brow;       // its row of chunk bases
+  int np, nch, m;
+  unsigned mk, mk1;      // masks of chunk m (bits left) and m + 1
+  int base, base1;
+  __device__ __forceinline__ void init(const Dev& d, int i) {
+    const int row = d.crow[i];
+    np = d.Npad;
+    mcol = d.nmask + i;
+    brow = d.cbase + (size_t)row * d.cap;
+    nch = d.cnch[row];
+    m = 0;
+    mk = nch > 0 ? __ldg(mcol) : 0u;
+    base = nch > 0 ? __ldg(brow) : 0;
+    mk1 = nch > 1 ? __ldg(mcol + (size_t)np) : 0u;
+    base1 = nch > 1 ? __ldg(brow + 1) : 0;
+  }
+  __device__ __forceinline__ int next() {
+    while (mk == 0u) {
+      if (++m >= nch) return -1;  // past the last candidate
+      mk = mk1;
+      base = base1;
+      if (m + 1 < nch) {
+        mk1 = __ldg(mcol + (size_t)(m + 1) * np);
+        base1 = __ldg(brow + m + 1);
+      } else {
+        mk1 = 0u;
+      }
+    }
+    const int q = __ffs(mk) - 1;
+    mk &= mk - 1u;
+    return base + q;
+  }
+};
+
 // True once a kernel before this one reported a failure: the step's state-changing kernels
 // then return at entry.  The flag word is read past L1 (it is written by atomics in L2).  In
 // kernels whose warps cooperate, lane 0's reading is taken by the whole warp.

@@ -314,12 +314,24 @@ __device__ __forceinline__ void density_epilogue(const Dev& d, int i, const BoxP
 
 // One warp per cell: the cell's particles (<= 32 per round) test the candidates of the
 // 3^d neighbour cells, staged 32 at a time in shared memory as float offsets from the
-// cell corner, and append hits to their own lists.  Candidate ranges come from the
-// reference-semantics cell_start / cell_end, so the candidate set and order are the
-// reference's (kernel_densities.cu:52-163), stale ranges included.  The float test uses
-// a slightly enlarged cutoff; consumers apply the exact test.  A particle whose own
-// (unclamped) cell differs from its sort cell (x exactly at L) is listed separately
-// with its own neighbour cells.
+// cell corner.  Candidate ranges come from the reference-semantics cell_start / cell_end,
+// so the candidate set and order are the reference's (kernel_densities.cu:52-163), stale
+// ranges included.  The float test uses a slightly enlarged cutoff; consumers apply the
+// exact test.
+//
+// The lists are hit masks, not indices.  Every particle of a cell tests the same sequence
+// of candidate chunks (up to 32 consecutive slots of one neighbour cell), so a cell's
+// chunk bases are stored once per cell (cbase, the cell's row of the chunk table, with the
+// chunk count in cnch) and each particle stores one 32-bit mask per chunk (bit q: slot
+// base + q is a candidate), chunk-major: nmask[k * Npad + i], so the warp's 32 masks of a
+// chunk are one coalesced 128-byte store.  The masks list the neighbours in the same order
+// as an index list would (chunk order, then bit order), at 4 bytes per 32 candidates
+// instead of 4 bytes per neighbour, and the build needs no per-lane append loop.
+//
+// A particle whose own (unclamped) cell differs from its sort cell (x exactly at L) has
+// other neighbour cells: it gets a row of its own in the chunk table (rows Ctot and up,
+// taken by an atomic counter), built by the whole warp with ballots.  crow[i] names the
+// row of particle i.
 //
 // (Summing the density over the hits inside this kernel was measured slower than the
 // separate k_density pass: the per-lane hit loops diverge and the warp runs the FP64
@@ -327,7 +339,8 @@ __device__ __forceinline__ void density_epilogue(const Dev& d, int i, const BoxP
 //
 // TPC (threads per cell) is 32 or 16.  With 16, each half-warp works on its own cell:
 // 2D cells at overlap 4 hold about 16 particles, so a whole warp per cell leaves half of
-// its lanes idle.  The lists are the same either way (same candidates, same order).
+// its lanes idle.  The neighbours are the same either way (same candidates, same order);
+// chunks are then 16 slots long.
 //
 // Blocks of 4 warps, measured against 8 (128^3 list build 1.66 vs 1.88 ms; 2D ensemble
 // 1.15 vs 1.19 ms, with the test loop not unrolled).
@@ -383,16 +396,6 @@ __global__ void __launch_bounds__(kListWarps * 32) k_build_lists(Dev d) {
   __shared__ __align__(16) float stage_x[kListWarps][32];
   __shared__ __align__(16) float stage_y[kListWarps][32];
   __shared__ __align__(16) float stage_z[kListWarps][32];
-  // each lane's pending list entries, one column per lane (conflict-free single-entry
-  // writes); a lane writes its row in groups of 8 entries, whole 32-byte sectors, instead
-  // of one scattered 4-byte store per entry
-  __shared__ int pending[kListWarps][8][32];
-  // each lane's hit mask per tested chunk, and the chunk's first slot per group; decoded in
-  // one loop per lane after the cells, so that the warp runs the busiest lane's total hit
-  // count rather than the busiest lane's count of every chunk
-  constexpr int kMaxCh = 32;
-  __shared__ unsigned hmask[kListWarps][kMaxCh][32];
-  __shared__ int hbase[kListWarps][kMaxCh][2];
   const int w = threadIdx.x >> 5, lane = threadIdx.x & 31;
   if (step_aborted_warp(d)) return;
   const int sub = lane / TPC, gl = lane % TPC;  // group within the warp, lane within the group
@@ -415,14 +418,40 @@ __global__ void __launch_bounds__(kListWarps * 32) k_build_lists(Dev d) {
   const double oy = cy * p.cell_size[1] - (p.wall ? p.wall_width : 0.0);
   const double oz = DIM == 3 ? cz * p.cell_size[2] : 0.0;
   const float cut2 = (float)p.list_cut2;
-  const int cap = d.cap;
+  const int cap = d.cap;  // chunks per row of the chunk table
+  const size_t Np = d.Npad;
   auto warp_max = [](int v) {
 #pragma unroll
     for (int o = 16; o > 0; o >>= 1) v = max(v, __shfl_xor_sync(SPH_FULL, v, o));
     return v;
   };
   const int span = warp_max(end - beg);
-  int maxcnt = 0;
+  int maxch = 0;  // the most chunks any row of this warp needed
+  // the neighbour cells' candidate ranges: with a warp per cell, lane q loads those of
+  // neighbour cell q up front (all 3^d loads in flight at once) and the loop takes them
+  // by shuffle; a half-warp group loads them as it goes
+  constexpr int kNZ = DIM == 3 ? 3 : 1;
+  int rs = 0, re = -1;
+  if (TPC == 32 && live && lane < 9 * kNZ) {
+    const int ddx = lane / (3 * kNZ) - 1, ddy = (lane / kNZ) % 3 - 1;
+    const int ddz = DIM == 3 ? lane % 3 - 1 : 0;
+    int nx = cx + ddx, ny = cy + ddy, nz = cz + ddz;
+    if (nx < 0) nx += N0;
+    if (nx >= N0) nx -= N0;
+    if (DIM == 3) {
+      if (nz < 0) nz += N2;
+      if (nz >= N2) nz -= N2;
+    }
+    if (!p.wall) {
+      if (ny < 0) ny += N1;
+      if (ny >= N1) ny -= N1;
+    }
+    if (ny >= 0 && ny < N1) {
+      const int nc = p.cell0 + (DIM == 3 ? (nz * N1 + ny) * N0 + nx : ny * N0 + nx);
+      rs = d.cell_start[nc] + p.slot0;
+      re = d.cell_end[nc] + p.slot0;
+    }
+  }
   for (int t0 = 0; t0 < span; t0 += TPC) {
     const int i = beg + t0 + gl;
     const bool active = i < end;
@@ -444,63 +473,13 @@ __global__ void __launch_bounds__(kListWarps * 32) k_build_lists(Dev d) {
       }
     }
     const bool listed = active && !odd && !lost;
+    const bool own_row = active && !odd;  // masks go to the cell's row
     const f32x2 xi2 = f2_pack(xi, xi), yi2 = f2_pack(yi, yi), zi2 = f2_pack(zi, zi);
     const f32x2 cut22 = f2_pack(cut2, cut2);
-    int* rowp = d.nbr + (size_t)(active ? i : 0) * cap;
-    int cnt = 0;
-    int* pend = &pending[w][0][lane];
-    // entries base .. base + 7 of this lane's row from its pending column (base % 8 == 0:
-    // rows start 32-byte aligned, cap % 8 == 0)
-    auto flush8 = [&](int base) {
-      int4* dst = reinterpret_cast<int4*>(rowp + base);
-      dst[0] = make_int4(pend[0], pend[32], pend[64], pend[96]);
-      dst[1] = make_int4(pend[128], pend[160], pend[192], pend[224]);
-    };
-    int nmask = 0;  // chunks recorded since the last decode (warp-uniform)
-    // this lane's recorded hits, chunk by chunk and bit by bit (divergent, no warp sync)
-    auto decode = [&]() {
-      // one flat loop: an iteration either moves to this lane's next chunk or appends one
-      // hit, so lanes run independently and the warp runs the busiest lane's total
-      int m = 0;
-      unsigned mk = nmask > 0 ? hmask[w][0][lane] : 0u;
-      while (m < nmask) {
-        if (mk == 0u) {
-          if (++m < nmask) mk = hmask[w][m][lane];
-          continue;
-        }
-        const int q = __ffs(mk) - 1;
-        mk &= mk - 1u;
-        const int k8 = cnt & 7;
-        pend[k8 * 32] = hbase[w][m][sub] + q;
-        if (k8 == 7 && cnt < cap) flush8(cnt - 7);  // entries cnt - 7 .. cnt
-        ++cnt;
-      }
-    };
-    // the neighbour cells' candidate ranges: with a warp per cell, lane q loads those of
-    // neighbour cell q up front (all 3^d loads in flight at once) and the loop takes them
-    // by shuffle; a half-warp group loads them as it goes
-    constexpr int kNZ = DIM == 3 ? 3 : 1;
-    int rs = 0, re = -1;
-    if (TPC == 32 && live && lane < 9 * kNZ) {
-      const int ddx = lane / (3 * kNZ) - 1, ddy = (lane / kNZ) % 3 - 1;
-      const int ddz = DIM == 3 ? lane % 3 - 1 : 0;
-      int nx = cx + ddx, ny = cy + ddy, nz = cz + ddz;
-      if (nx < 0) nx += N0;
-      if (nx >= N0) nx -= N0;
-      if (DIM == 3) {
-        if (nz < 0) nz += N2;
-        if (nz >= N2) nz -= N2;
-      }
-      if (!p.wall) {
-        if (ny < 0) ny += N1;
-        if (ny >= N1) ny -= N1;
-      }
-      if (ny >= 0 && ny < N1) {
-        const int nc = p.cell0 + (DIM == 3 ? (nz * N1 + ny) * N0 + nx : ny * N0 + nx);
-        rs = d.cell_start[nc] + p.slot0;
-        re = d.cell_end[nc] + p.slot0;
-      }
-    }
+    unsigned* mcol = d.nmask + (own_row ? i : 0);  // this particle's masks, stride Npad
+    int* brow = d.cbase + (size_t)cl * cap;        // the cell's chunk bases
+    int cnt = 0;                                   // this lane's candidates
+    int kc = 0;                                    // chunks of the cell's row (group-uniform)
     for (int ddx = -1; ddx <= 1; ++ddx)
       for (int ddy = -1; ddy <= 1; ++ddy)
         for (int ddz = (DIM == 3 ? -1 : 0); ddz <= (DIM == 3 ? 1 : 0); ++ddz) {
@@ -551,42 +530,38 @@ __global__ void __launch_bounds__(kListWarps * 32) k_build_lists(Dev d) {
             if (TPC == 16 || listed) {
 #pragma unroll 1
               for (int q = 0; q < m; q += 4) {
-                const float4 cx = *reinterpret_cast<const float4*>(stx + q);
-                const float4 cy = *reinterpret_cast<const float4*>(sty + q);
-                const float4 cz = DIM == 3 ? *reinterpret_cast<const float4*>(stz + q)
-                                           : make_float4(0.f, 0.f, 0.f, 0.f);
-                hits = list_test2<DIM>(hits, xi2, yi2, zi2, cut22, cx.x, cx.y, cy.x, cy.y, cz.x,
-                                       cz.y);
-                hits = list_test2<DIM>(hits, xi2, yi2, zi2, cut22, cx.z, cx.w, cy.z, cy.w, cz.z,
-                                       cz.w);
+                const float4 cx4 = *reinterpret_cast<const float4*>(stx + q);
+                const float4 cy4 = *reinterpret_cast<const float4*>(sty + q);
+                const float4 cz4 = DIM == 3 ? *reinterpret_cast<const float4*>(stz + q)
+                                            : make_float4(0.f, 0.f, 0.f, 0.f);
+                hits = list_test2<DIM>(hits, xi2, yi2, zi2, cut22, cx4.x, cx4.y, cy4.x, cy4.y,
+                                       cz4.x, cz4.y);
+                hits = list_test2<DIM>(hits, xi2, yi2, zi2, cut22, cx4.z, cx4.w, cy4.z, cy4.w,
+                                       cz4.z, cz4.w);
               }
               // first candidate was shifted in first: reverse into bit q = candidate q
               hits = m > 0 ? __brev(hits) >> (32 - m) : 0u;
               if (TPC == 16) hits &= (listed && n > 0) ? (0xFFFFFFFFu >> (32 - n)) : 0u;
             }
-            // recorded for the decode after the cells (candidate order is kept)
-            hmask[w][nmask][lane] = hits;
-            if (gl == 0) hbase[w][nmask][sub] = c0;
-            if (++nmask == kMaxCh) {
-              __syncwarp();
-              decode();
-              nmask = 0;
+            if (k < nch) {  // a chunk of this group's row
+              if (kc < cap) {
+                if (own_row) mcol[(size_t)kc * Np] = hits;
+                if (t0 == 0 && gl == 0 && live) brow[kc] = c0;
+              }
+              cnt += __popc(hits);
+              ++kc;
             }
-            __syncwarp();
+            __syncwarp();  // the stage is refilled by the next chunk
           }
         }
-    __syncwarp();
-    decode();
-    __syncwarp();  // the mask table is refilled by the next round
-    // the last, partial group (the entries past cnt in it are never read); rows hold cap
-    // entries, cap a multiple of 8, so a group below cap lies wholly inside the row
-    if ((cnt & 7) != 0 && cnt < cap) flush8(cnt & ~7);
-    if (active && !odd) {
+    if (own_row) {
       d.nbr_cnt[i] = cnt;
-      maxcnt = max(maxcnt, cnt);
+      d.crow[i] = cl;
     }
-    // particles exactly on the upper box edge: their own neighbour cells, the whole warp
-    // testing one such particle's candidates at a time
+    if (t0 == 0 && gl == 0 && live) d.cnch[cl] = min(kc, cap);
+    maxch = max(maxch, kc);
+    // particles exactly on the upper box edge: their own neighbour cells in a row of their
+    // own, the whole warp testing one such particle's candidates at a time
     unsigned odd_mask = __ballot_sync(SPH_FULL, active && odd);
     while (odd_mask) {
       const int l = __ffs(odd_mask) - 1;
@@ -594,6 +569,20 @@ __global__ void __launch_bounds__(kListWarps * 32) k_build_lists(Dev d) {
       // the particle and its cell's geometry, from the lane that holds it
       const int ti = __shfl_sync(SPH_FULL, i, l);
       const int tb = __shfl_sync(SPH_FULL, b, l);
+      int orow = 0;
+      if (lane == 0) orow = atomicAdd(d.odd_count, 1);
+      orow = __shfl_sync(SPH_FULL, orow, 0);
+      if (orow >= d.odd_cap) {
+        // no row left: no neighbours, and the lists are reported too short (they grow)
+        if (lane == 0) {
+          d.nbr_cnt[ti] = 0;
+          d.crow[ti] = cl;
+          raise_status(d, kStatCapacity, 0, kPhaseLists);
+        }
+        continue;
+      }
+      const int trow = d.Ctot + orow;
+      int* tbrow = d.cbase + (size_t)trow * cap;
       const BoxParams& tp = d.box[tb];
       const double4 xt = d.pos[ti];
       int ax = 0, ay = 0, az = 0;
@@ -604,7 +593,7 @@ __global__ void __launch_bounds__(kListWarps * 32) k_build_lists(Dev d) {
       const double toz = DIM == 3 ? az * tp.cell_size[2] : 0.0;
       const float tcut2 = (float)tp.list_cut2;
       const float txi = (float)(xt.x - tox), tyi = (float)(xt.y - toy), tzi = (float)(xt.z - toz);
-      int tcnt = 0;
+      int tcnt = 0, tk = 0;
       for (int ddx = -1; ddx <= 1; ++ddx)
         for (int ddy = -1; ddy <= 1; ++ddy)
           for (int ddz = (DIM == 3 ? -1 : 0); ddz <= (DIM == 3 ? 1 : 0); ++ddz) {
@@ -638,20 +627,27 @@ __global__ void __launch_bounds__(kListWarps * 32) k_build_lists(Dev d) {
                 hit = r2 < tcut2;
               }
               const unsigned hits = __ballot_sync(SPH_FULL, hit);
-              const int pos = tcnt + __popc(hits & ((1u << lane) - 1u));
-              if (hit && pos < cap) d.nbr[(size_t)ti * cap + pos] = j;
+              if (lane == 0 && tk < cap) {
+                d.nmask[(size_t)tk * Np + ti] = hits;
+                tbrow[tk] = c0;
+              }
               tcnt += __popc(hits);
+              ++tk;
             }
           }
-      if (lane == 0) d.nbr_cnt[ti] = tcnt;
-      maxcnt = max(maxcnt, tcnt);
+      if (lane == 0) {
+        d.nbr_cnt[ti] = tcnt;
+        d.crow[ti] = trow;
+        d.cnch[trow] = min(tk, cap);
+      }
+      maxch = max(maxch, tk);
     }
   }
-  // warp max of the counts -> capacity check
-  maxcnt = warp_max(maxcnt);
-  if (lane == 0 && maxcnt > 0) {
-    atomicMax(&d.err_info[kErrMaxCount], maxcnt);
-    if (maxcnt > cap) raise_status(d, kStatCapacity, 0, kPhaseLists);
+  // warp max of the chunk counts -> capacity check
+  maxch = warp_max(maxch);
+  if (lane == 0 && maxch > 0) {
+    atomicMax(&d.err_info[kErrMaxCount], maxch);
+    if (maxch > cap) raise_status(d, kStatCapacity, 0, kPhaseLists);
   }
 }
 
@@ -716,25 +712,18 @@ __global__ void k_density(Dev d) {
   const T rcutsq = (T)p.rcutsq;
   const T rcut_inv = (T)p.rcut_inv, cw = (T)p.cw;
   const V xi = ld_pos<DIM>(P + i);
-  const int n = min(d.nbr_cnt[i], d.cap);
-  // the particle's list row, read four indices at a time one batch ahead
-  const int4* __restrict__ row = reinterpret_cast<const int4*>(d.nbr + (size_t)i * d.cap);
+  const int n = d.nbr_cnt[i];
+  NbrIter it;
+  it.init(d, i);
   T dens = T(0), comp = T(0);  // comp: Kahan compensation of a float sum
-  int4 nxt = n > 0 ? __ldg(&row[0]) : make_int4(0, 0, 0, 0);
-  for (int k0 = 0; k0 < n; k0 += 4) {
-    const int4 cur = nxt;
-    if (k0 + 4 < n) nxt = __ldg(&row[(k0 >> 2) + 1]);
-    const int m = min(4, n - k0);
-#pragma unroll
-    for (int q = 0; q < 4; ++q) {
-      if (q >= m) break;
-      const int j = q == 0 ? cur.x : q == 1 ? cur.y : q == 2 ? cur.z : cur.w;
-      const T w = density_term<T, DIM>(xi, ld_pos<DIM>(P + j), L, h, p.wall, rcutsq, rcut_inv, cw);
-      if constexpr (Compensated<T>::on)
-        kahan_add(dens, comp, w);
-      else
-        dens = dens + w;
-    }
+  for (int k = 0; k < n; ++k) {
+    const int j = it.next();
+    if (j < 0) break;
+    const T w = density_term<T, DIM>(xi, ld_pos<DIM>(P + j), L, h, p.wall, rcutsq, rcut_inv, cw);
+    if constexpr (Compensated<T>::on)
+      kahan_add(dens, comp, w);
+    else
+      dens = dens + w;
   }
   density_epilogue<T, DIM>(d, i, p, (double)dens - (double)comp);
 }
@@ -803,8 +792,11 @@ __global__ void __launch_bounds__(kDensWarps * 32) k_density_cells(Dev d) {
     const int i = beg + t0 + lane;
     const bool active = i < end;
     const V xi = active ? ld_pos<DIM>(P + i) : V{};
-    const int n = active ? min(d.nbr_cnt[i], d.cap) : 0;
-    const int* __restrict__ row = d.nbr + (size_t)(active ? i : 0) * d.cap;
+    const int n = active ? d.nbr_cnt[i] : 0;
+    NbrIter it;
+    it.init(d, active ? i : beg);
+    // the next list entry not yet summed (-1: none left)
+    int jn = n > 0 ? it.next() : -1;
     T dens = T(0), comp = T(0);  // comp: Kahan compensation of a float sum
     auto add = [&](const V& xj) {
       const T wv = density_term<T, DIM>(xi, xj, L, h, p.wall, rcutsq, rcut_inv, cw);
@@ -846,8 +838,8 @@ __global__ void __launch_bounds__(kDensWarps * 32) k_density_cells(Dev d) {
       // this lane's list entries that fall in the phase's ranges, in list order
       int qc = 0;
       int qs = rtab[w][0][0], qe = rtab[w][0][1], qo = rtab[w][0][2];
-      while (k < n) {
-        const int j = __ldg(&row[k]);
+      while (k < n && jn >= 0) {
+        const int j = jn;
         while (qc < kPerPh && (j < qs || j > qe)) {
           if (++qc < kPerPh) {
             qs = rtab[w][qc][0];
@@ -867,11 +859,15 @@ __global__ void __launch_bounds__(kDensWarps * 32) k_density_cells(Dev d) {
         }
         add(xj);
         ++k;
+        jn = k < n ? it.next() : -1;
       }
       __syncwarp();  // the tile and the range table are refilled by the next phase
     }
     // entries from no staged range: global reads, still in list order
-    for (; k < n; ++k) add(ld_pos<DIM>(P + __ldg(&row[k])));
+    for (; k < n && jn >= 0; ++k) {
+      add(ld_pos<DIM>(P + jn));
+      jn = k + 1 < n ? it.next() : -1;
+    }
     if (active) density_epilogue<T, DIM>(d, i, p, (double)dens - (double)comp);
   }
 }
@@ -998,7 +994,6 @@ struct PairWalk {
   using Rec = typename RecFor<T, DIM>::type;
   const Dev& d;
   const Rec* __restrict__ rec;
-  const int4* __restrict__ row;  // the lane's list row, four indices per load
   int4* sb;                      // the warp's staging rows
   int lane, i, n, nmax;
   const BoxParams& p;
@@ -1009,15 +1004,12 @@ struct PairWalk {
 
 // One position per step: the copies for position k + 1 are in flight while k is evaluated.
 template <typename T, int DIM>
-__device__ __forceinline__ void pair_walk1(const PairWalk<T, DIM>& W, PairAcc<T, DIM>& acc) {
+__device__ __forceinline__ void pair_walk1(const PairWalk<T, DIM>& W, NbrIter& it,
+                                           PairAcc<T, DIM>& acc) {
   using Rec = typename RecFor<T, DIM>::type;
   using St = PairStage<Rec>;
   const int n = W.n, lane = W.lane;
-  // `cur` holds the batch of the position being staged, `nxt` the following one (loaded
-  // four positions ahead)
-  int4 cur = n > 0 ? __ldg(&W.row[0]) : make_int4(-1, -1, -1, -1);
-  int4 nxt = n > 4 ? __ldg(&W.row[1]) : make_int4(-1, -1, -1, -1);
-  int jc = n > 0 ? cur.x : -1;
+  int jc = n > 0 ? it.next() : -1;
   // 2D records carry no type word: the neighbour's is read from the type array one
   // position ahead, with its record's copy
   int tc = DIM == 2 && jc >= 0 ? __ldg(&W.d.tinfo[jc]) : 0;
@@ -1025,12 +1017,7 @@ __device__ __forceinline__ void pair_walk1(const PairWalk<T, DIM>& W, PairAcc<T,
   cp_async_commit();
   for (int k = 0; k < W.nmax; ++k) {
     const int k1 = k + 1;
-    if ((k1 & 3) == 0) {
-      cur = nxt;
-      if (k1 + 4 < n) nxt = __ldg(&W.row[(k1 >> 2) + 1]);
-    }
-    const int q = k1 & 3;
-    const int jn = k1 < n ? (q == 0 ? cur.x : q == 1 ? cur.y : q == 2 ? cur.z : cur.w) : -1;
+    const int jn = k1 < n ? it.next() : -1;
     if (k1 < W.nmax) stage_records<Rec>(W.sb + (k1 & 1) * St::kRows, W.rec, jn, lane);
     const int tn = DIM == 2 && jn >= 0 ? __ldg(&W.d.tinfo[jn]) : 0;
     cp_async_commit();
@@ -1051,13 +1038,13 @@ __device__ __forceinline__ void pair_walk1(const PairWalk<T, DIM>& W, PairAcc<T,
 // Two positions per step: the copies for positions k + 2, k + 3 are in flight while k and
 // k + 1 are evaluated, side by side where every lane's partners there are fluid.
 template <typename T, int DIM>
-__device__ __forceinline__ void pair_walk2(const PairWalk<T, DIM>& W, PairAcc<T, DIM>& acc) {
+__device__ __forceinline__ void pair_walk2(const PairWalk<T, DIM>& W, NbrIter& it,
+                                           PairAcc<T, DIM>& acc) {
   using Rec = typename RecFor<T, DIM>::type;
   using St = PairStage<Rec>;
   const int n = W.n, lane = W.lane;
-  int4 cur = n > 0 ? __ldg(&W.row[0]) : make_int4(-1, -1, -1, -1);
-  int4 nxt = n > 4 ? __ldg(&W.row[1]) : make_int4(-1, -1, -1, -1);
-  int ja = n > 0 ? cur.x : -1, jb = n > 1 ? cur.y : -1;
+  int ja = n > 0 ? it.next() : -1;
+  int jb = n > 1 ? it.next() : -1;
   int ta = DIM == 2 && ja >= 0 ? __ldg(&W.d.tinfo[ja]) : 0;
   int tb = DIM == 2 && jb >= 0 ? __ldg(&W.d.tinfo[jb]) : 0;
   stage_records<Rec>(W.sb, W.rec, ja, lane);
@@ -1065,13 +1052,8 @@ __device__ __forceinline__ void pair_walk2(const PairWalk<T, DIM>& W, PairAcc<T,
   cp_async_commit();
   for (int k = 0; k < W.nmax; k += 2) {
     const int k2 = k + 2;
-    if ((k2 & 3) == 0) {
-      cur = nxt;
-      if (k2 + 4 < n) nxt = __ldg(&W.row[(k2 >> 2) + 1]);
-    }
-    const bool hi = (k2 & 2) != 0;
-    const int jna = k2 < n ? (hi ? cur.z : cur.x) : -1;
-    const int jnb = k2 + 1 < n ? (hi ? cur.w : cur.y) : -1;
+    const int jna = k2 < n ? it.next() : -1;
+    const int jnb = k2 + 1 < n ? it.next() : -1;
     if (k2 < W.nmax) {
       int4* nbuf = W.sb + ((k2 >> 1) & 1) * 2 * St::kRows;
       stage_records<Rec>(nbuf, W.rec, jna, lane);
@@ -1135,16 +1117,17 @@ __global__ void __launch_bounds__(PairShape<T, DIM>::kWarps * 32, PairShape<T, D
   load_own<T, DIM, MODE>(d, is, ti, rec[is], o);
   PairAcc<T, DIM> acc;
   acc.zero();
-  const int n = active ? min(d.nbr_cnt[i], d.cap) : 0;
+  const int n = active ? d.nbr_cnt[i] : 0;
   int nmax = n;
 #pragma unroll
   for (int s = 16; s > 0; s >>= 1) nmax = max(nmax, __shfl_xor_sync(SPH_FULL, nmax, s));
-  const PairWalk<T, DIM> W{d, rec, reinterpret_cast<const int4*>(d.nbr + (size_t)is * d.cap),
-                           &stage[w][0][0], lane, i, n, nmax, p, pp, cv, o};
+  NbrIter it;
+  it.init(d, is);
+  const PairWalk<T, DIM> W{d, rec, &stage[w][0][0], lane, i, n, nmax, p, pp, cv, o};
   if constexpr (Sh::kILP == 2)
-    pair_walk2<T, DIM>(W, acc);
+    pair_walk2<T, DIM>(W, it, acc);
   else
-    pair_walk1<T, DIM>(W, acc);
+    pair_walk1<T, DIM>(W, it, acc);
   if (active) pair_store<T, DIM, MODE, EXT>(d, i, p, o, acc);
 }
 
@@ -1686,6 +1669,8 @@ int launch_reorder(const Launch& L, bool permute_forces) {
 
 int launch_build_lists_dim(const Launch& L, int dim) {
   if (L.d.Ctot == 0) return 0;
+  // own rows of the chunk table are handed out from zero by every build
+  if (cudaMemsetAsync(L.d.odd_count, 0, sizeof(int), S(L)) != cudaSuccess) return check(L);
   const bool half = L.list_tpc == 16;
   const int nb = blocks(L.d.Ctot, kListWarps * (half ? 2 : 1));
   constexpr int nt = kListWarps * 32;

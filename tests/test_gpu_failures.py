@@ -21,10 +21,11 @@ STATE = ["x", "y", "z", "vx", "vy", "vz", "fx", "fy", "fz", "dens", "press", "cx
          "cyy", "cxz", "cyz", "czz"]
 
 
-def converging_box(workdir, A=30.0):
+def converging_box(workdir, A=60.0):
     """16^3 periodic box whose fluid converges on the plane y = 0.5 (vy = -A (y - 0.5)): the
-    lattice there is compressed along y by about A t, so after some steps more neighbours
-    come within the list cutoff than at the start."""
+    lattice is compressed along y by about A t, so after some 30 steps cells hold more than
+    32 particles where they held fewer, and rows need more candidate chunks than at the
+    start (46 -> 54 by a kinematic estimate)."""
     spec = dict(N=(16, 16, 16), L=(1.0, 1.0, 1.0), dim=3, overlap=3.0, dt=1e-4)
     lat = os.path.join(workdir, "input_lattice")
     sph_input.write_input(lat, **spec)
@@ -44,13 +45,13 @@ def test_list_overflow_inside_a_call_resumes(workdir, precision, use_graph):
     ref = sph_b200.System(inp, [pp], precision=precision, use_graph=use_graph)
     ref.step(0)
     need0 = ref.neighbour_lists()["max_used"]
-    # lists exactly long enough (rounded up to a multiple of 8) for the initial search
+    # lists exactly long enough for the initial search
     tight = sph_b200.System(inp, [pp], precision=precision, use_graph=use_graph,
                             nbr_capacity=need0)
     tight.step(0)
     st0 = tight.neighbour_lists()
-    assert st0["grown"] == 0 and st0["capacity"] < need0 + 8, st0
-    nsteps = 30
+    assert st0["grown"] == 0 and st0["capacity"] == need0, st0
+    nsteps = 40
     ref.step(nsteps)
     tight.step(nsteps)  # one call: the overflow comes in one of its steps
     ref.synchronize()
