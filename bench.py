@@ -108,7 +108,8 @@ class ClockSampler:
 
     Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
          "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
-         "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+         "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap,"
+         "utilization.gpu")
 
     def __init__(self, device):
         self.device = device
@@ -140,7 +141,7 @@ class ClockSampler:
     def summary(self):
         if not self.proc:
             return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
-        sm, smax, reasons = [], [], set()
+        sm, smax, busy, reasons = [], [], [], set()
         names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
         with open(self.path) as f:
             for line in f:
@@ -148,17 +149,26 @@ class ClockSampler:
                 if len(p) < 9:
                     continue
                 try:
-                    sm.append(float(p[1]))
-                    smax.append(float(p[2]))
+                    clk, top = float(p[1]), float(p[2])
                 except ValueError:
                     continue
+                sm.append(clk)
+                smax.append(top)
+                try:
+                    util = float(p[9]) if len(p) > 9 else 100.0
+                except ValueError:
+                    util = 100.0
+                if util > 0:
+                    busy.append(clk)
                 for k, name in enumerate(names):
                     if p[5 + k].lower() == "active":
                         reasons.add(name)
         if not sm:
             return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["no samples"]}
-        return {"sm_mhz": statistics.median(sm), "sm_max_mhz": max(smax),
-                "samples": len(sm), "reasons": sorted(reasons)}
+        # the median over the samples in which the GPU was busy (a sampled process that also
+        # reads its input spends part of its time with the GPU idle, at idle clocks)
+        return {"sm_mhz": statistics.median(busy or sm), "sm_max_mhz": max(smax),
+                "samples": len(sm), "busy_samples": len(busy), "reasons": sorted(reasons)}
 
 
 def write_workload(d, lattice=128):

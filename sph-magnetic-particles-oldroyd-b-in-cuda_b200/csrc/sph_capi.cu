@@ -343,10 +343,22 @@ sph_status regrow_lists(sph_ctx* c) {
 }
 
 sph_status search_checked(sph_ctx* c) {
+  const bool permute = c->forces_live;
   if (ph_search(c)) return cuda_fail(c, "neighbours_search");
-  sph_status s = check_device(c);
-  if (s == SPH_ERR_CAPACITY) s = regrow_lists(c);
-  return s;
+  unsigned st = 0;
+  int info[kErrInfoLen] = {0};
+  if (!read_device_status(c, &st, info)) return cuda_fail(c, "device status");
+  if (st == 0) return SPH_OK;
+  cudaMemsetAsync(c->d.status, 0, sizeof(unsigned), c->stream);
+  if (info[kErrPhase] == kPhaseHash) {
+    // the hash stopped the search before its reorder: the state is still in the previous
+    // order, in the buffers the host swapped away from
+    swap_state(c, permute);
+    c->pos_dirty = true;
+  }
+  if (st == kStatCapacity) return regrow_lists(c);
+  c->pos_dirty = true;
+  return status_of(c, st, info, "");
 }
 
 sph_status ensure_lists(sph_ctx* c) {
@@ -1139,6 +1151,9 @@ sph_status sph_profile_phases(sph_ctx* c, int nsteps, double* ms) {
     sph_status s = do_initial(c);
     if (s != SPH_OK) return s;
   }
+  // the profiled steps are checked as one call (a failure stops them where it is found)
+  const long long step0 = c->host_step;
+  const int parity0 = c->parity;
   cudaEvent_t ev[SPH_NUM_PHASES + 1];
   for (auto& e : ev) cudaEventCreate(&e);
   std::vector<double> acc(SPH_NUM_PHASES, 0.0);
@@ -1194,7 +1209,11 @@ sph_status sph_profile_phases(sph_ctx* c, int nsteps, double* ms) {
   drop_graphs(c);  // the buffer parity may have changed
   if (bad) return cuda_fail(c, "profile_phases");
   for (int k = 0; k < SPH_NUM_PHASES; ++k) ms[k] = acc[k] / nsteps;
-  return check_device(c);
+  c->call_open = true;
+  c->call_step0 = step0;
+  c->call_parity0 = parity0;
+  c->call_target = c->host_step;
+  return settle_call(c);
 }
 
 // ---- state access ----

@@ -5,7 +5,8 @@ sources and run on a B200 by tests/golden/make_golden.py) after the initial forc
 after 1 and 5 steps.  The oracle must reproduce every integer array (cell hash, sorted
 order, cell ranges, colloid coarse grid) exactly and every real field within 1e-10 of
 the field group's scale; the observed differences are at 1e-12 and below and come from
-the FMA contractions of nvcc and the CUDA math library.
+the FMA contractions of nvcc and the CUDA math library.  The 64^2 Kolmogorov case is also
+stored after its full 2000 steps, where the bound is 1e-9.
 
 Exception, by design: the reference's 3D colloid velocity-gradient branch writes past a
 two-element array (src/kernel_vel_gradients.cu:463-466, 567-570), so its gradients next
@@ -24,6 +25,9 @@ from conftest import COLLOID_GROUPS, GROUPS, group_error
 
 HERE = os.path.dirname(os.path.abspath(__file__))
 TOL = 1e-10
+# after the 2000 steps of the 64^2 Kolmogorov case the FMA-contraction differences have
+# grown to about 1e-10 in the forces (residuals of cancelling pressure terms)
+TOL_LONG = 1e-9
 INTS = ["type", "particle_cell", "particle_index", "cell_start", "cell_end"]
 CINTS = ["coll_cell", "coll_index", "coll_cell_start", "coll_cell_end"]
 
@@ -52,7 +56,7 @@ def test_oracle_matches_reference_build(name, workdir):
             if not fl:
                 continue
             err = group_error(o.field, lambda f: g["s%d_%s" % (s, f)], fl, norm, dim)
-            assert err <= TOL, (name, s, gname, err)
+            assert err <= (TOL if s <= 5 else TOL_LONG), (name, s, gname, err)
         if "fx_wall" in keys:
             err = group_error(o.field, lambda f: g["s%d_%s" % (s, f)],
                               ["fx_wall", "fy_wall", "fz_wall"], "max", dim if dim == 3 else 2)
