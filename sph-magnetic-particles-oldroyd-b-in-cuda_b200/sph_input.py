@@ -115,7 +115,8 @@ def suspension_centres(n, R, rcut, seed, L=(1.0, 1.0, 1.0), min_dist=2.2, tries=
     return tuple(out)
 
 
-def suspension_spec(N=96, n_colloids=32, seed=11, nsteps=2000, tau_repulsion=1.0):
+def suspension_spec(N=96, n_colloids=32, seed=11, nsteps=2000, tau_repulsion=1.0,
+                    F0_repulsion=10.0, F0_magnetic=5.0):
     """The 3D suspension of rotating magnetic colloids between walls at rest: N^3 lattice,
     L = 1, overlap 3, Oldroyd-B (tau 1, np 100, kT 0.01, eta 0.1, rho 1, c 10, P0 0),
     n_colloids colloids of radius 4 dx (density 1, moving), repulsion cut-on 2.05 R
@@ -132,5 +133,6 @@ def suspension_spec(N=96, n_colloids=32, seed=11, nsteps=2000, tau_repulsion=1.0
                 tau=1.0, dt=2e-5, Nsteps=nsteps, N_colloids=n_colloids, coll_R=R,
                 coll_rho=1.0, coll_move=0,
                 coll_x=suspension_centres(n_colloids, R, rcut, seed),
-                coll_repulsion_cuton=0.05 * R, F0_repulsion=10.0, tau_repulsion=tau_repulsion,
-                cutoff_magnetic=6.0 * R, F0_magnetic=5.0, omega_magnetic=2.0 * np.pi)
+                coll_repulsion_cuton=0.05 * R, F0_repulsion=F0_repulsion,
+                tau_repulsion=tau_repulsion, cutoff_magnetic=6.0 * R, F0_magnetic=F0_magnetic,
+                omega_magnetic=2.0 * np.pi)
