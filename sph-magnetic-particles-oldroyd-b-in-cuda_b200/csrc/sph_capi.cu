@@ -126,9 +126,9 @@ void swap_state(sph_ctx* c, bool with_forces) {
   c->parity ^= 1;
 }
 
-// Chunks per row of the neighbour chunk table: every neighbour cell of a cell (3^d of them)
-// gives its particles in chunks of up to 16 (a half warp per cell) or 32 slots.  Sized for
-// cells holding 1.5 times the lattice's particles per cell, in chunks of 16.
+// Neighbour-list capacity: chunks with hits per particle.  A particle's candidates come
+// from the 3^d neighbour cells in chunks of up to 16 (a half warp per cell) or 32 slots;
+// sized for cells holding 1.5 times the lattice's particles per cell, in chunks of 16.
 int derived_capacity(const std::vector<HostBox>& boxes, int dim) {
   int worst = 1;
   for (const HostBox& hb : boxes) {
@@ -141,13 +141,8 @@ int derived_capacity(const std::vector<HostBox>& boxes, int dim) {
   return worst;
 }
 
-// Own rows of the chunk table for particles listed from their own cells (on the upper box
-// edge): rare, so a small table.
-int derived_odd_rows(int Ntot) { return 256 + Ntot / 1024; }
-
-// Allocates the neighbour-list buffers for `cap` chunks per row and `odd_cap` own rows,
-// replacing any earlier ones.
-bool alloc_lists(sph_ctx* c, int cap, int odd_cap) {
+// Allocates the neighbour-list entries for `cap` chunks per particle, replacing earlier ones.
+bool alloc_lists(sph_ctx* c, int cap) {
   Dev& d = c->d;
   auto replace = [&](auto** ptr, size_t n) {
     using T = std::remove_pointer_t<std::remove_reference_t<decltype(*ptr)>>;
@@ -164,12 +159,8 @@ bool alloc_lists(sph_ctx* c, int cap, int odd_cap) {
     *ptr = static_cast<T*>(q);
     return true;
   };
-  const size_t rows = (size_t)d.Ctot + odd_cap;
-  if (!replace(&d.nmask, (size_t)cap * d.Npad) || !replace(&d.cbase, rows * cap) ||
-      !replace(&d.cnch, rows))
-    return false;
+  if (!replace(&d.nchunk, (size_t)cap * d.Npad)) return false;
   d.cap = cap;
-  d.odd_cap = odd_cap;
   return true;
 }
 
@@ -221,16 +212,11 @@ void drop_graphs(sph_ctx* c) {
     }
 }
 
-// Grows the chunk table to hold `needed` chunks per row (with headroom), and its own rows
-// to hold the last list build's count of particles listed from their own cells.
+// Grows the lists to hold `needed` chunks per particle, with headroom.
 sph_status grow_capacity(sph_ctx* c, int needed) {
-  int odd = 0;
-  if (cudaMemcpy(&odd, c->d.odd_count, sizeof(int), cudaMemcpyDeviceToHost) != cudaSuccess)
-    return cuda_fail(c, "list statistics");
-  const int cap = std::max(needed + needed / 4 + 2, c->d.cap + (needed > c->d.cap ? 4 : 0));
-  const int odd_cap = odd > c->d.odd_cap ? 2 * odd + 64 : c->d.odd_cap;
+  const int cap = std::max(needed + needed / 4 + 2, c->d.cap + 4);
   cudaStreamSynchronize(c->stream);
-  if (!alloc_lists(c, cap, odd_cap)) return fail(c, SPH_ERR_NOMEM, "cannot grow neighbour lists");
+  if (!alloc_lists(c, cap)) return fail(c, SPH_ERR_NOMEM, "cannot grow neighbour lists");
   c->cap_grown++;
   drop_graphs(c);
   return SPH_OK;
@@ -738,12 +724,12 @@ sph_status sph_create_ensemble(int nboxes, const sph_input* inputs,
     ok = ok && dalloc(c, &r, Np);
     d.rec = r;
   }
-  ok = ok && dalloc(c, &d.nbr_cnt, Np) && dalloc(c, &d.crow, Np) && dalloc(c, &d.odd_count, 1);
+  ok = ok && dalloc(c, &d.nbr_cnt, Np) && dalloc(c, &d.nbr_nch, Np);
   ok = ok && dalloc(c, &d.key_by_gid, Np) && dalloc(c, &d.keys, Np) && dalloc(c, &d.vals, Np);
   ok = ok && dalloc(c, &d.keys_alt, Np) && dalloc(c, &d.vals_alt, Np);
   ok = ok && dalloc(c, &d.cell_begin, Ctot + 1) && dalloc(c, &d.cell_start, Ctot);
   ok = ok && dalloc(c, &d.cell_end, Ctot) && dalloc(c, &d.cell_box, Ctot);
-  ok = ok && alloc_lists(c, list_cap, derived_odd_rows(d.Ntot));
+  ok = ok && alloc_lists(c, list_cap);
   ok = ok && dalloc(c, &d.walls_list, nwl) && dalloc(c, &d.wall_seg, nwall + 1);
   ok = ok && dalloc(c, &d.wall_f, 3 * std::max(nwall, 1));
   d.nwallchunks = nwchunk;

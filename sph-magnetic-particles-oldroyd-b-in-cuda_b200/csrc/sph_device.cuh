@@ -147,41 +147,34 @@ __device__ __forceinline__ void raise_status(const Dev& d, unsigned bit, int inf
   }
 }
 
-// One particle's neighbour candidates in list order, decoded from the hit masks the list
-// build writes: row r = crow[i] of the chunk table holds cnch[r] chunk bases
-// (cbase[r * cap + k]); the particle's mask of chunk k is nmask[k * Npad + i], bit q meaning
-// slot base + q.  Candidates come chunk by chunk and, inside a chunk, by increasing slot,
-// which is the reference's candidate order.  The next chunk's mask and base are loaded one
-// chunk ahead.  next() gives nbr_cnt[i] candidates, then -1.
+// One particle's neighbour candidates in list order, decoded from the chunk entries the list
+// build writes: nchunk[k * Npad + i] = (first slot, hit mask) of the particle's k-th chunk
+// with hits (nbr_nch[i] of them), bit q of the mask meaning slot first + q.  Candidates come
+// chunk by chunk and, inside a chunk, by increasing slot: the reference's candidate order.
+// Every stored chunk has a hit, so moving to the next one never loops; its entry is loaded
+// one chunk ahead.  next() gives nbr_cnt[i] candidates, then -1.
 struct NbrIter {
-  const unsigned* mcol;  // this particle's masks, stride np
-  const int* brow;       // its row of chunk bases
-  int np, nch, m;
-  unsigned mk, mk1;      // masks of chunk m (bits left) and m + 1
-  int base, base1;
+  const int2* col;  // this particle's entries, stride np
+  int np, nch, c;   // c: the current chunk
+  unsigned mk;      // its bits not yet taken
+  int base;
+  int2 nxt;         // entry of chunk c + 1
   __device__ __forceinline__ void init(const Dev& d, int i) {
-    const int row = d.crow[i];
     np = d.Npad;
-    mcol = d.nmask + i;
-    brow = d.cbase + (size_t)row * d.cap;
-    nch = d.cnch[row];
-    m = 0;
-    mk = nch > 0 ? __ldg(mcol) : 0u;
-    base = nch > 0 ? __ldg(brow) : 0;
-    mk1 = nch > 1 ? __ldg(mcol + (size_t)np) : 0u;
-    base1 = nch > 1 ? __ldg(brow + 1) : 0;
+    col = d.nchunk + i;
+    nch = d.nbr_nch[i];
+    c = 0;
+    const int2 e0 = nch > 0 ? __ldg(col) : make_int2(0, 0);
+    base = e0.x;
+    mk = (unsigned)e0.y;
+    nxt = nch > 1 ? __ldg(col + (size_t)np) : make_int2(0, 0);
   }
   __device__ __forceinline__ int next() {
-    while (mk == 0u) {
-      if (++m >= nch) return -1;  // past the last candidate
-      mk = mk1;
-      base = base1;
-      if (m + 1 < nch) {
-        mk1 = __ldg(mcol + (size_t)(m + 1) * np);
-        base1 = __ldg(brow + m + 1);
-      } else {
-        mk1 = 0u;
-      }
+    if (mk == 0u) {
+      if (++c >= nch) return -1;  // past the last candidate
+      base = nxt.x;
+      mk = (unsigned)nxt.y;
+      if (c + 1 < nch) nxt = __ldg(col + (size_t)(c + 1) * np);
     }
     const int q = __ffs(mk) - 1;
     mk &= mk - 1u;

@@ -147,7 +147,7 @@ static_assert(sizeof(RecF2) == 32, "RecF2 layout");
 // Device pointers, passed to kernels by value.
 struct Dev {
   int Ntot, Npad, nboxes, Ctot, ncoll, nwallseg;
-  int cap;  // chunks per row of the neighbour chunk table
+  int cap;  // neighbour-list capacity: chunks with hits per particle
   const BoxParams* box;
   double4* pos;  // x, y, z, mass
   double4* vel;  // vx, vy, vz, 0
@@ -169,17 +169,11 @@ struct Dev {
   double* dcdt_b;  // a force evaluation and the half-kick that consumes it
   double* gradv; // 9 x Npad: xx xy xz yx yy yz zx zy zz
   void* rec;     // RecD or RecF per slot
-  // neighbour candidates as hit masks (k_build_lists): per particle one 32-bit mask per
-  // chunk of up to 32 consecutive candidate slots, chunk-major (nmask[k * Npad + i]); the
-  // chunk bases of a cell's particles are shared, one row of the chunk table per cell
-  // (rows 0..Ctot-1) plus rows for particles listed from their own cells (Ctot and up)
-  unsigned* nmask;  // cap x Npad
-  int* cbase;       // (Ctot + odd_cap) x cap: first slot of each chunk of a row
-  int* cnch;        // (Ctot + odd_cap): chunks in a row
-  int* crow;        // Npad: the row of each particle
-  int* odd_count;   // own rows taken by the last list build
-  int odd_cap;      // own rows available
-  int* nbr_cnt;     // per slot: candidates (set bits over the particle's masks)
+  // neighbour candidates (k_build_lists): per particle, for every chunk of up to 32
+  // consecutive candidate slots in which it has a hit, (first slot, hit mask), chunk-major
+  int2* nchunk;     // cap x Npad: nchunk[k * Npad + i]
+  int* nbr_nch;     // per slot: chunks stored
+  int* nbr_cnt;     // per slot: candidates (set bits over the particle's chunks)
   int* key_by_gid;
   int* keys;     // sorted keys
   int* vals;     // sorted values (global ids)

@@ -319,19 +319,17 @@ __device__ __forceinline__ void density_epilogue(const Dev& d, int i, const BoxP
 // ranges included.  The float test uses a slightly enlarged cutoff; consumers apply the
 // exact test.
 //
-// The lists are hit masks, not indices.  Every particle of a cell tests the same sequence
-// of candidate chunks (up to 32 consecutive slots of one neighbour cell), so a cell's
-// chunk bases are stored once per cell (cbase, the cell's row of the chunk table, with the
-// chunk count in cnch) and each particle stores one 32-bit mask per chunk (bit q: slot
-// base + q is a candidate), chunk-major: nmask[k * Npad + i], so the warp's 32 masks of a
-// chunk are one coalesced 128-byte store.  The masks list the neighbours in the same order
-// as an index list would (chunk order, then bit order), at 4 bytes per 32 candidates
-// instead of 4 bytes per neighbour, and the build needs no per-lane append loop.
+// The lists are chunks with hit masks, not indices.  Candidates come in chunks of up to 32
+// consecutive slots of one neighbour cell; for every chunk in which it has a hit, a particle
+// stores one 8-byte entry (the chunk's first slot, a 32-bit mask whose bit q means slot
+// first + q is a candidate), chunk-major: nchunk[k * Npad + i], so that consumers walking
+// their lists in step read neighbouring words.  Decoding the entries in order, bit by bit,
+// gives the neighbours in the order of an index list (the reference's candidate order), at
+// 8 bytes per chunk with hits (about 20 in 3D) instead of 4 bytes per neighbour (about
+// 108), and the build needs no per-lane append loop: a chunk's hits are one store.
 //
 // A particle whose own (unclamped) cell differs from its sort cell (x exactly at L) has
-// other neighbour cells: it gets a row of its own in the chunk table (rows Ctot and up,
-// taken by an atomic counter), built by the whole warp with ballots.  crow[i] names the
-// row of particle i.
+// other neighbour cells; its whole warp tests its candidates with ballots.
 //
 // (Summing the density over the hits inside this kernel was measured slower than the
 // separate k_density pass: the per-lane hit loops diverge and the warp runs the FP64
@@ -418,7 +416,7 @@ __global__ void __launch_bounds__(kListWarps * 32) k_build_lists(Dev d) {
   const double oy = cy * p.cell_size[1] - (p.wall ? p.wall_width : 0.0);
   const double oz = DIM == 3 ? cz * p.cell_size[2] : 0.0;
   const float cut2 = (float)p.list_cut2;
-  const int cap = d.cap;  // chunks per row of the chunk table
+  const int cap = d.cap;  // chunks with hits a particle can store
   const size_t Np = d.Npad;
   auto warp_max = [](int v) {
 #pragma unroll
@@ -426,7 +424,7 @@ __global__ void __launch_bounds__(kListWarps * 32) k_build_lists(Dev d) {
     return v;
   };
   const int span = warp_max(end - beg);
-  int maxch = 0;  // the most chunks any row of this warp needed
+  int maxch = 0;  // the most chunks with hits any particle of this warp had
   // the neighbour cells' candidate ranges: with a warp per cell, lane q loads those of
   // neighbour cell q up front (all 3^d loads in flight at once) and the loop takes them
   // by shuffle; a half-warp group loads them as it goes
@@ -473,13 +471,11 @@ __global__ void __launch_bounds__(kListWarps * 32) k_build_lists(Dev d) {
       }
     }
     const bool listed = active && !odd && !lost;
-    const bool own_row = active && !odd;  // masks go to the cell's row
     const f32x2 xi2 = f2_pack(xi, xi), yi2 = f2_pack(yi, yi), zi2 = f2_pack(zi, zi);
     const f32x2 cut22 = f2_pack(cut2, cut2);
-    unsigned* mcol = d.nmask + (own_row ? i : 0);  // this particle's masks, stride Npad
-    int* brow = d.cbase + (size_t)cl * cap;        // the cell's chunk bases
-    int cnt = 0;                                   // this lane's candidates
-    int kc = 0;                                    // chunks of the cell's row (group-uniform)
+    int2* col = d.nchunk + (listed ? i : 0);  // this particle's chunks, stride Npad
+    int cnt = 0;                              // this lane's candidates
+    int kc = 0;                               // this lane's chunks with hits
     for (int ddx = -1; ddx <= 1; ++ddx)
       for (int ddy = -1; ddy <= 1; ++ddy)
         for (int ddz = (DIM == 3 ? -1 : 0); ddz <= (DIM == 3 ? 1 : 0); ++ddz) {
@@ -543,25 +539,21 @@ __global__ void __launch_bounds__(kListWarps * 32) k_build_lists(Dev d) {
               hits = m > 0 ? __brev(hits) >> (32 - m) : 0u;
               if (TPC == 16) hits &= (listed && n > 0) ? (0xFFFFFFFFu >> (32 - n)) : 0u;
             }
-            if (k < nch) {  // a chunk of this group's row
-              if (kc < cap) {
-                if (own_row) mcol[(size_t)kc * Np] = hits;
-                if (t0 == 0 && gl == 0 && live) brow[kc] = c0;
-              }
+            if (hits != 0u) {  // a chunk with hits: (first slot, mask) in the next entry
+              if (kc < cap) col[(size_t)kc * Np] = make_int2(c0, (int)hits);
               cnt += __popc(hits);
               ++kc;
             }
             __syncwarp();  // the stage is refilled by the next chunk
           }
         }
-    if (own_row) {
+    if (active && !odd) {
       d.nbr_cnt[i] = cnt;
-      d.crow[i] = cl;
+      d.nbr_nch[i] = min(kc, cap);
     }
-    if (t0 == 0 && gl == 0 && live) d.cnch[cl] = min(kc, cap);
     maxch = max(maxch, kc);
-    // particles exactly on the upper box edge: their own neighbour cells in a row of their
-    // own, the whole warp testing one such particle's candidates at a time
+    // particles exactly on the upper box edge: their own neighbour cells, the whole warp
+    // testing one such particle's candidates at a time
     unsigned odd_mask = __ballot_sync(SPH_FULL, active && odd);
     while (odd_mask) {
       const int l = __ffs(odd_mask) - 1;
@@ -569,20 +561,6 @@ __global__ void __launch_bounds__(kListWarps * 32) k_build_lists(Dev d) {
       // the particle and its cell's geometry, from the lane that holds it
       const int ti = __shfl_sync(SPH_FULL, i, l);
       const int tb = __shfl_sync(SPH_FULL, b, l);
-      int orow = 0;
-      if (lane == 0) orow = atomicAdd(d.odd_count, 1);
-      orow = __shfl_sync(SPH_FULL, orow, 0);
-      if (orow >= d.odd_cap) {
-        // no row left: no neighbours, and the lists are reported too short (they grow)
-        if (lane == 0) {
-          d.nbr_cnt[ti] = 0;
-          d.crow[ti] = cl;
-          raise_status(d, kStatCapacity, 0, kPhaseLists);
-        }
-        continue;
-      }
-      const int trow = d.Ctot + orow;
-      int* tbrow = d.cbase + (size_t)trow * cap;
       const BoxParams& tp = d.box[tb];
       const double4 xt = d.pos[ti];
       int ax = 0, ay = 0, az = 0;
@@ -627,18 +605,16 @@ __global__ void __launch_bounds__(kListWarps * 32) k_build_lists(Dev d) {
                 hit = r2 < tcut2;
               }
               const unsigned hits = __ballot_sync(SPH_FULL, hit);
-              if (lane == 0 && tk < cap) {
-                d.nmask[(size_t)tk * Np + ti] = hits;
-                tbrow[tk] = c0;
+              if (hits != 0u) {
+                if (lane == 0 && tk < cap) d.nchunk[(size_t)tk * Np + ti] = make_int2(c0, (int)hits);
+                tcnt += __popc(hits);
+                ++tk;
               }
-              tcnt += __popc(hits);
-              ++tk;
             }
           }
       if (lane == 0) {
         d.nbr_cnt[ti] = tcnt;
-        d.crow[ti] = trow;
-        d.cnch[trow] = min(tk, cap);
+        d.nbr_nch[ti] = min(tk, cap);
       }
       maxch = max(maxch, tk);
     }
@@ -1669,8 +1645,6 @@ int launch_reorder(const Launch& L, bool permute_forces) {
 
 int launch_build_lists_dim(const Launch& L, int dim) {
   if (L.d.Ctot == 0) return 0;
-  // own rows of the chunk table are handed out from zero by every build
-  if (cudaMemsetAsync(L.d.odd_count, 0, sizeof(int), S(L)) != cudaSuccess) return check(L);
   const bool half = L.list_tpc == 16;
   const int nb = blocks(L.d.Ctot, kListWarps * (half ? 2 : 1));
   constexpr int nt = kListWarps * 32;
