@@ -191,14 +191,21 @@ def particles_file(input_path):
 
 
 SUSPENSION_NAME = ("suspension3d_96: 96^3 Oldroyd-B fluid between walls at rest with 32 rotating "
-                   "magnetic colloids of radius 4 dx (sph_input.suspension_spec, seed 11)")
+                   "magnetic colloids of radius 4 dx (sph_input.suspension_spec, seed 11), "
+                   "F0_repulsion 1e-3, F0_magnetic 5e-4")
 SUSPENSION_METRIC = "particle-steps/s (96^3 magnetic suspension, 32 colloids)"
+# The amplitudes as the configuration writes them (F0_repulsion 10, F0_magnetic 5) drive the
+# colloids of radius 4 dx to speeds of hundreds of box lengths per unit time (the magnetic
+# force is F0 / r^4 with r in box units, ~1e3 per pair at contact on a colloid of mass 3e-4)
+# and one colloid leaves the box at step 154, where the reference would trap on its cell
+# range check; scaled by 1e-4 the run is stable for its 2000 steps (colloid speeds below 1.2).
+SUSPENSION_F0 = dict(F0_repulsion=1e-3, F0_magnetic=5e-4)
 
 
 def write_suspension(d, lattice=96):
     """The 3D magnetic suspension input in directory d (lattice start, no restart file)."""
     path = os.path.join(d, "input")
-    sph_input.write_input(path, **sph_input.suspension_spec(N=lattice))
+    sph_input.write_input(path, **sph_input.suspension_spec(N=lattice, **SUSPENSION_F0))
     return path
 
 

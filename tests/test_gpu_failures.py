@@ -17,22 +17,22 @@ import sph_b200
 import sph_input
 
 pytestmark = pytest.mark.gpu
-STATE = ["x", "y", "z", "vx", "vy", "vz", "fx", "fy", "fz", "dens", "press", "cxx", "cxy",
-         "cyy", "cxz", "cyz", "czz"]
+STATE = ["x", "y", "vx", "vy", "fx", "fy", "dens", "press", "cxx", "cxy", "cyy"]
 
 
 def converging_box(workdir, A=60.0):
-    """16^3 periodic box whose fluid converges on the plane y = 0.5 (vy = -A (y - 0.5)): the
-    lattice is compressed along y by about A t, so after some 30 steps cells hold more than
-    32 particles where they held fewer, and rows need more candidate chunks than at the
-    start (46 -> 54 by a kinematic estimate)."""
-    spec = dict(N=(16, 16, 16), L=(1.0, 1.0, 1.0), dim=3, overlap=3.0, dt=1e-4)
+    """64^2 periodic 2D box at overlap 4 (cells of exactly 4 x 4 = 16 particles) whose fluid
+    converges on the line y = 0.5 (vy = -A (y - 0.5)): the lattice is compressed along y by
+    about A t, so after some 30 steps cells hold a fifth row.  With a half warp per cell
+    (candidate chunks of 16 slots) a cell of more than 16 particles gives its neighbours two
+    chunks instead of one, and particles need more chunks than at the start."""
+    spec = dict(N=(64, 64), L=(1.0, 1.0), dim=2, overlap=4.0, dt=1e-4)
     lat = os.path.join(workdir, "input_lattice")
     sph_input.write_input(lat, **spec)
     a, info = sph_b200.host_setup(lat)
     a = dict(a, vy=-A * (a["y"] - 0.5))
     pp = os.path.join(workdir, "input_particles.in")
-    sph_b200.write_restart(pp, 3, a)
+    sph_b200.write_restart(pp, 2, a)
     inp = os.path.join(workdir, "input")
     sph_input.write_input(inp, new_sim=1, **spec)
     return inp, pp
@@ -42,16 +42,19 @@ def converging_box(workdir, A=60.0):
                                                  ("fp64", False)])
 def test_list_overflow_inside_a_call_resumes(workdir, precision, use_graph):
     inp, pp = converging_box(workdir)
-    ref = sph_b200.System(inp, [pp], precision=precision, use_graph=use_graph)
+    # the reference run: lists far longer than needed
+    ref = sph_b200.System(inp, [pp], precision=precision, use_graph=use_graph, nbr_capacity=64)
+    ref.set_tuning(list_threads_per_cell=16)
     ref.step(0)
     need0 = ref.neighbour_lists()["max_used"]
     # lists exactly long enough for the initial search
     tight = sph_b200.System(inp, [pp], precision=precision, use_graph=use_graph,
                             nbr_capacity=need0)
+    tight.set_tuning(list_threads_per_cell=16)
     tight.step(0)
     st0 = tight.neighbour_lists()
     assert st0["grown"] == 0 and st0["capacity"] == need0, st0
-    nsteps = 40
+    nsteps = 50
     ref.step(nsteps)
     tight.step(nsteps)  # one call: the overflow comes in one of its steps
     ref.synchronize()

@@ -76,3 +76,46 @@ def test_suspension96_fp64_matches_oracle(workdir):
     assert e.info()["step"] == 10, errs
     e.close()
     o.close()
+
+
+# Mixed precision against FP64 after the 2000 steps of the configuration, with the magnetic
+# and repulsion amplitudes scaled by 1e-4 (F0_repulsion 1e-3, F0_magnetic 5e-4): as written
+# (10 and 5) the colloids reach hundreds of box lengths per unit time and one leaves the box
+# at step 154 in both precisions.  Bounds: about 3-10 times the errors measured on B200
+# (positions 9e-8 of L, colloid positions 3e-8, quaternions 1.4e-8, colloid velocities
+# 3.4e-6 and angular velocities 4.5e-6 of their scale, wall forces 1.6e-8, fluid velocities
+# 1.3e-5, density 6e-6, conformation 7e-6, forces 7.5e-6; torques, small residuals of large
+# cancelling fluid forces, 9.4e-4).
+TRAJ_TOL = dict(pos=1e-6, vel=2e-4, force=1e-4, dens=5e-5, press=5e-5, conf=1e-4, dcdt=5e-4,
+                cpos=3e-7, cvel=5e-5, comega=5e-5, cforce=1e-4, ctorque=1e-2, quat=2e-7,
+                walls=1e-6)
+
+
+def test_suspension96_mixed_follows_fp64_for_2000_steps(workdir):
+    spec = sph_input.suspension_spec(F0_repulsion=1e-3, F0_magnetic=5e-4)
+    inp = os.path.join(workdir, "input")
+    sph_input.write_input(inp, **spec)
+    a = sph_b200.System(inp, precision="fp64")
+    b = sph_b200.System(inp, precision="mixed")
+    a.step(2000)
+    b.step(2000)
+    a.synchronize()
+    b.synchronize()
+    assert a.info()["step"] == b.info()["step"] == 2000
+    errs = {}
+    for gname, (fields, norm) in GROUPS.items():
+        if gname != "grad":
+            errs[gname] = group_error(b.field, a.field, fields, norm, 3)
+    for gname, (fields, norm) in COLLOID_GROUPS.items():
+        errs[gname] = group_error(b.colloid_field, a.colloid_field, fields, norm, 3)
+    q = ["coll_quat0", "coll_quatx", "coll_quaty", "coll_quatz"]
+    errs["quat"] = max(float(np.abs(a.colloid_field(k) - b.colloid_field(k)).max()) for k in q)
+    wa, wb = a.wall_forces(), b.wall_forces()
+    errs["walls"] = float(np.abs(wa - wb).max() / np.abs(wa).max())
+    for k, v in errs.items():
+        assert v <= TRAJ_TOL[k], (k, v, errs)
+    # the colloids stay in the box, clear of the walls
+    y = a.colloid_field("coll_y")
+    assert np.all(np.isfinite(y)) and y.min() > 0.0 and y.max() < 1.0
+    a.close()
+    b.close()
