@@ -81,13 +81,13 @@ def test_suspension96_fp64_matches_oracle(workdir):
 # Mixed precision against FP64 after the 2000 steps of the configuration, with the magnetic
 # and repulsion amplitudes scaled by 1e-4 (F0_repulsion 1e-3, F0_magnetic 5e-4): as written
 # (10 and 5) the colloids reach hundreds of box lengths per unit time and one leaves the box
-# at step 154 in both precisions.  Bounds: about 3-10 times the errors measured on B200
+# at step 154 (FP64 engine).  Bounds: about 3-10 times the errors measured on B200
 # (positions 9e-8 of L, colloid positions 3e-8, quaternions 1.4e-8, colloid velocities
 # 3.4e-6 and angular velocities 4.5e-6 of their scale, wall forces 1.6e-8, fluid velocities
-# 1.3e-5, density 6e-6, conformation 7e-6, forces 7.5e-6; torques, small residuals of large
-# cancelling fluid forces, 9.4e-4).
+# 1.3e-5, density 6e-6, conformation 7e-6, forces 7.5e-6; colloid forces 8.3e-5 and torques
+# 9.4e-4, small residuals of large cancelling fluid forces).
 TRAJ_TOL = dict(pos=1e-6, vel=2e-4, force=1e-4, dens=5e-5, press=5e-5, conf=1e-4, dcdt=5e-4,
-                cpos=3e-7, cvel=5e-5, comega=5e-5, cforce=1e-4, ctorque=1e-2, quat=2e-7,
+                cpos=3e-7, cvel=5e-5, comega=5e-5, cforce=5e-4, ctorque=1e-2, quat=2e-7,
                 walls=1e-6)
 
 
