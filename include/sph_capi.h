@@ -81,9 +81,10 @@ typedef struct sph_options {
   int precision;    /* sph_precision                                                   */
   int device;       /* CUDA device ordinal                                             */
   int use_graph;    /* sph_step replays a captured CUDA graph of one step             */
-  int nbr_capacity; /* neighbour-list capacity in candidate chunks per cell (a chunk is
-                       up to 32 consecutive slots of one neighbour cell); 0 = derived
-                       from overlap and dim.  Lists grow when a build needs more. */
+  int nbr_capacity; /* neighbour-list capacity in candidate chunks per particle (a chunk
+                       is up to 32 consecutive slots of one neighbour cell in which the
+                       particle has a neighbour); 0 = derived from overlap and dim.
+                       Lists grow when a build needs more. */
   int init_on_device; /* 1: lattice boxes (new_sim 0) are built on the GPU -- sites,
                          colloid carving, wall layers, walls lists -- bit-identical to the
                          host set-up; colloid shells and restart files stay on the host */
@@ -225,8 +226,8 @@ sph_status sph_step(sph_ctx* ctx, int nsteps);
 sph_status sph_synchronize(sph_ctx* ctx);
 
 /* Neighbour-list statistics (no reference counterpart: the reference has no lists): the
-   capacity of a list row, the largest row the list builds have needed, and how many times
-   the lists have grown. */
+   capacity in candidate chunks per particle, the most chunks a particle has needed in the
+   list builds so far, and how many times the lists have grown. */
 sph_status sph_neighbour_lists(sph_ctx* ctx, int* capacity, int* max_used, int* grown);
 
 /* -------------------------------------------------------------- state access */

@@ -411,8 +411,8 @@ class System:
         return v.value
 
     def neighbour_lists(self):
-        """{'capacity', 'max_used', 'grown'}: candidate chunks a cell's list row holds, the
-        most chunks a row has needed so far, and how many times the lists have grown."""
+        """{'capacity', 'max_used', 'grown'}: candidate chunks a particle's list holds, the
+        most chunks a particle has needed so far, and how many times the lists have grown."""
         cap, used, grown = c_int(0), c_int(0), c_int(0)
         lib().sph_neighbour_lists.argtypes = [c_void_p, PI, PI, PI]
         self._ok(lib().sph_neighbour_lists(self._h, ctypes.byref(cap), ctypes.byref(used),

@@ -272,8 +272,8 @@ def test_forces_store_the_same_gradient_as_the_gradient_pass(name, workdir):
 
 @pytest.mark.parametrize("precision", ["fp64", "mixed"])
 def test_neighbour_capacity_grows(precision, workdir):
-    """Neighbour lists that start far too short (8 candidate chunks per cell where 27 are
-    needed) overflow, are detected on the device, grow and are rebuilt: the run is
+    """Neighbour lists that start far too short (8 candidate chunks per particle where about
+    20 are needed) overflow, are detected on the device, grow and are rebuilt: the run is
     bit-identical to one with the derived capacity, through the step graph and through the
     step methods."""
     mg.case_dir("colloids3d", workdir)
