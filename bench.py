@@ -740,7 +740,7 @@ def main():
     ap.add_argument("--e2e-steps", type=int, default=20)
     ap.add_argument("--pairs-traffic", type=float, default=None,
                     help="ncu DRAM bytes per k_pairs launch (default: the FP64 capture at "
-                         "96^3, 786.6 MB, scaled by particle count to the benchmark)")
+                         "96^3, 505.8 MB, scaled by particle count to the benchmark)")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-secondary", action="store_true",
                     help="skip the short mixed-precision, ensemble and surrogate figures that "
@@ -763,7 +763,7 @@ def main():
             and args.precision in (None, "fp64")):
         # dram__bytes_read.sum + dram__bytes_write.sum of one k_pairs launch at 96^3
         # (940,032 particles), scaled to the 2,195,456 particles of the benchmark
-        args.pairs_traffic = (722.4832e6 + 64.10752e6) * 2195456 / 940032
+        args.pairs_traffic = (386.815232e6 + 118.972928e6) * 2195456 / 940032
     if args.precision is None:
         args.precision = "mixed" if args.workload == "sweep" else "fp64"
     if args.warmup < 3:
