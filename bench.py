@@ -523,6 +523,10 @@ def run_ensemble(args, world, rank, local, dist, emit=True):
         ms_max = max_over_ranks(dist, ms, local)
         n_all = sum(sph_ensemble.box_cost(s, 1) for s in specs)
         value = n_all * args.steps / (ms_max * 1e-3)
+        # per-phase device times of the same step launched phase by phase (CUDA events between
+        # the phases): their sum against the graph-replayed step shows what the graph's launch
+        # gaps cost
+        phases = sysm.profile_phases(args.profile_steps)
         # e2e: every step one observables sample of every box, read back to the host
         e2e_steps = min(args.steps, args.e2e_steps)
         t0 = time.perf_counter()
@@ -565,6 +569,8 @@ def run_ensemble(args, world, rank, local, dist, emit=True):
                 "d2h_bytes_per_step": 512 * 4 * 8, "steps": e2e_steps},
         "gpu_launches": launches,
         "clocks": clk.summary(),
+        "phase_ms": phases,
+        "phase_sum_ms": sum(phases.values()),
     }
     if looped:
         line["looped_single_box"] = looped
