@@ -23,3 +23,20 @@ def test_sweep_line_is_json():
     assert json.loads(text)["unit"] == "points/h"
     assert line["value"] > 0 and line["accepted"] is True
     assert "2000 steps" in line["config"]["workload"]
+
+
+def test_single_box_workloads_write_their_inputs(tmp_path):
+    """The couette3d workload writes the seeded restart start beside its input; the
+    suspension96 workload writes the lattice input of config 3 with the scaled amplitudes."""
+    import bench
+
+    (tmp_path / "c").mkdir()
+    (tmp_path / "s").mkdir()
+    c = bench.WORKLOADS["couette3d"]
+    inp = c.write(str(tmp_path / "c"), lattice=12)
+    assert bench.particles_file(inp) is not None and "new_sim 1" in open(inp).read()
+    s = bench.WORKLOADS["suspension96"]
+    inp = s.write(str(tmp_path / "s"), lattice=96)
+    text = open(inp).read()
+    assert bench.particles_file(inp) is None
+    assert text.count("coll_x ") == 32 and "F0_magnetic 0.0005" in text
