@@ -149,7 +149,8 @@ __device__ __forceinline__ void raise_status(const Dev& d, unsigned bit, int inf
 
 // One particle's neighbour candidates in list order, decoded from the chunk entries the list
 // build writes: nchunk[k * Npad + i] = (first slot, hit mask) of the particle's k-th chunk
-// with hits (nbr_nch[i] of them), bit q of the mask meaning slot first + q.  Candidates come
+// with hits (nbr_nch[i] of them), bit 31 - q of the mask meaning slot first + q (the first
+// candidate in the highest bit, so that a count of leading zeros gives its offset).  Candidates come
 // chunk by chunk and, inside a chunk, by increasing slot: the reference's candidate order.
 // Every stored chunk has a hit, so moving to the next one never loops; its entry is loaded
 // one chunk ahead.  next() gives nbr_cnt[i] candidates, then -1.  It has no branch: the
@@ -180,8 +181,8 @@ struct NbrIter {
     const bool ld = r && c + 1 < nch;
     const int2* pn = col + (size_t)(c + 1) * np;
     if (ld) nxt = __ldg(pn);
-    const int q = __ffs(mk) - 1;
-    mk &= mk - 1u;
+    const int q = __clz(mk);  // 32 only past the last candidate, where the shift gives 0
+    mk ^= q < 32 ? 0x80000000u >> q : 0u;
     return c < nch ? base + q : -1;
   }
 };

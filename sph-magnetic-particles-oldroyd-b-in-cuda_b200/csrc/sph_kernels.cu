@@ -321,7 +321,7 @@ __device__ __forceinline__ void density_epilogue(const Dev& d, int i, const BoxP
 //
 // The lists are chunks with hit masks, not indices.  Candidates come in chunks of up to 32
 // consecutive slots of one neighbour cell; for every chunk in which it has a hit, a particle
-// stores one 8-byte entry (the chunk's first slot, a 32-bit mask whose bit q means slot
+// stores one 8-byte entry (the chunk's first slot, a 32-bit mask whose bit 31 - q means slot
 // first + q is a candidate), chunk-major: nchunk[k * Npad + i], so that consumers walking
 // their lists in step read neighbouring words.  Decoding the entries in order, bit by bit,
 // gives the neighbours in the order of an index list (the reference's candidate order), at
@@ -536,9 +536,10 @@ __global__ void __launch_bounds__(kListWarps * 32) k_build_lists(Dev d) {
                 hits = list_test2<DIM>(hits, xi2, yi2, zi2, ncut22, cx4.x, cy4.x, cz4.x);
                 hits = list_test2<DIM>(hits, xi2, yi2, zi2, ncut22, cx4.y, cy4.y, cz4.y);
               }
-              // first candidate was shifted in first: reverse into bit q = candidate q
-              hits = m > 0 ? __brev(hits) >> (32 - m) : 0u;
-              if (TPC == 16) hits &= (listed && n > 0) ? (0xFFFFFFFFu >> (32 - n)) : 0u;
+              // first candidate was shifted in first: align it to bit 31 (bit 31 - q is
+              // candidate q, the consumers' order of leading zeros)
+              hits = m > 0 ? hits << (32 - m) : 0u;
+              if (TPC == 16) hits &= (listed && n > 0) ? ~(0xFFFFFFFFu >> n) : 0u;
             }
             if (hits != 0u) {  // a chunk with hits: (first slot, mask) in the next entry
               if (kc < cap) col[(size_t)kc * Np] = make_int2(c0, (int)hits);
@@ -605,7 +606,7 @@ __global__ void __launch_bounds__(kListWarps * 32) k_build_lists(Dev d) {
                 }
                 hit = r2 < tcut2;
               }
-              const unsigned hits = __ballot_sync(SPH_FULL, hit);
+              const unsigned hits = __brev(__ballot_sync(SPH_FULL, hit));
               if (hits != 0u) {
                 if (lane == 0 && tk < cap) d.nchunk[(size_t)tk * Np + ti] = make_int2(c0, (int)hits);
                 tcnt += __popc(hits);
