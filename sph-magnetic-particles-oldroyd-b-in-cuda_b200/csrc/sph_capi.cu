@@ -743,6 +743,8 @@ sph_status sph_create_ensemble(int nboxes, const sph_input* inputs,
   ok = ok && dalloc(c, &d.mag, 3 * nboxes) && dalloc(c, &d.ke, nboxes);
   ok = ok && dalloc(c, &d.step, 1) && dalloc(c, &d.status, 1) &&
        dalloc(c, &d.err_info, kErrInfoLen);
+  // positions not yet looked at by a search: the pair passes keep the minimum image
+  if (ok) cudaMemsetAsync(d.err_info + kPosOutside, 1, sizeof(int), c->stream);
   ok = ok && dalloc(c, &c->scratch, Np) && dalloc(c, &c->iscratch, Np);
   c->sort.hist_len = (int)sort_hist_len(Ntot, c->key_bits);
   ok = ok && dalloc(c, &c->sort.hist, (size_t)c->sort.hist_len);

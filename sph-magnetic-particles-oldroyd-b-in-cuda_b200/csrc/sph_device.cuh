@@ -66,9 +66,12 @@ __device__ __forceinline__ T sph_gradw(T r, T rcut_inv, T c_gradw) {
 
 // Minimum image as the reference writes it: subtract L above L/2, add L below -L/2
 // (kernel_densities.cu:90-110).  y is periodic only without walls; z only in 3D.
-template <typename T, int DIM>
+// WRAP false: the separation is taken as it is (for particles clear of the periodic faces,
+// see clear_of_faces, where the shifts change no pair inside the cutoff).
+template <typename T, int DIM, bool WRAP = true>
 __device__ __forceinline__ void min_image(T& rx, T& ry, T& rz, const T L[3], const T h[3],
                                           int wall) {
+  if constexpr (!WRAP) return;
   if (rx > h[0]) rx -= L[0];
   if (rx < -h[0]) rx += L[0];
   if (!wall) {
@@ -79,6 +82,19 @@ __device__ __forceinline__ void min_image(T& rx, T& ry, T& rz, const T L[3], con
     if (rz > h[2]) rz -= L[2];
     if (rz < -h[2]) rz += L[2];
   }
+}
+
+// |r|^2 with explicit roundings, rx^2 then + ry^2 then + rz^2 by fused multiply-adds: the
+// compiler may contract a plain expression differently in each pass that inlines it, and
+// the passes with and without the minimum image (and the density's two forms) must agree
+// bit for bit.
+__device__ __forceinline__ double norm2(double rx, double ry, double rz, bool three) {
+  const double s = __fma_rn(ry, ry, __dmul_rn(rx, rx));
+  return three ? __fma_rn(rz, rz, s) : s;
+}
+__device__ __forceinline__ float norm2(float rx, float ry, float rz, bool three) {
+  const float s = __fmaf_rn(ry, ry, __fmul_rn(rx, rx));
+  return three ? __fmaf_rn(rz, rz, s) : s;
 }
 
 // Cell of a position as kernel_cell_list.cu:15-63 computes it (with its clamp rules).
@@ -197,6 +213,38 @@ __device__ __forceinline__ bool step_aborted_warp(const Dev& d) {
   unsigned v = 0u;
   if ((threadIdx.x & 31) == 0) v = *(volatile const unsigned*)d.status;
   return (__shfl_sync(0xffffffffu, v, 0) & kStatAbortMask) != 0u;
+}
+
+// A position outside [0, L] along a periodic axis of its box (or not finite).
+__device__ __forceinline__ bool outside_periodic(const BoxParams& p, double x, double y,
+                                                 double z) {
+  return !(x >= 0.0 && x <= p.L[0]) || (p.wall == 0 && !(y >= 0.0 && y <= p.L[1])) ||
+         (p.dim == 3 && !(z >= 0.0 && z <= p.L[2]));
+}
+__device__ __forceinline__ void mark_outside(const Dev& d) { d.err_info[kPosOutside] = 1; }
+
+// A particle at least 1.0625 rcut from every periodic face of its box.  While every position
+// lies in [0, L] along the periodic axes (err_info[kPosOutside] clear), the minimum image
+// changes no pair of such a particle that the sums take: a neighbour within the cutoff is
+// never across a face, and a pair whose plain separation along an axis exceeds L/2 fails the
+// cutoff both unshifted (L/2 > rcut) and shifted (then at least the margin, more than rcut,
+// since the particle is that far from the face).  The pair passes take the separations of
+// warps of such particles without the shifts: the same bits, fewer dependent operations.
+template <typename T, int DIM>
+__device__ __forceinline__ bool clear_of_faces(const BoxParams& p, T x, T y, T z) {
+  const T m = (T)(1.0625 * p.rcut);
+  bool in = x >= m && x <= (T)p.L[0] - m;
+  if (DIM == 3) in = in && z >= m && z <= (T)p.L[2] - m;
+  if (!p.wall) in = in && y >= m && y <= (T)p.L[1] - m;
+  return in;
+}
+// Whether a whole warp may drop the minimum image (every lane passes `clear`); lane 0's
+// reading of the flag is taken by the whole warp.
+__device__ __forceinline__ bool warp_plain_image(const Dev& d, bool clear) {
+  int v = 0;
+  if ((threadIdx.x & 31) == 0) v = *(volatile const int*)(d.err_info + kPosOutside);
+  v = __shfl_sync(0xffffffffu, v, 0);
+  return __all_sync(0xffffffffu, clear) && v == 0;
 }
 
 
@@ -510,14 +558,14 @@ __device__ __forceinline__ void load_own(const Dev& d, int i, int ti, const Rec&
 }
 
 // Separation r = x_i - x_j under the minimum image; returns |r|^2.
-template <typename T, int DIM, typename Rec>
+template <typename T, int DIM, bool WRAP, typename Rec>
 __device__ __forceinline__ T pair_sep(const PairParams<T, DIM>& pp, int wall,
                                       const PairOwn<T, DIM>& o, const Rec& rj, T r[3]) {
   r[0] = o.x - (T)rj.x;
   r[1] = o.y - (T)rj.y;
   r[2] = DIM == 3 ? o.z - (T)rec_z<DIM>(rj) : T(0);
-  min_image<T, DIM>(r[0], r[1], r[2], pp.L, pp.h, wall);
-  return DIM == 3 ? r[0] * r[0] + r[1] * r[1] + r[2] * r[2] : r[0] * r[0] + r[1] * r[1];
+  min_image<T, DIM, WRAP>(r[0], r[1], r[2], pp.L, pp.h, wall);
+  return norm2(r[0], r[1], r[2], DIM == 3);
 }
 
 // 1/|r|, the kernel slope gw = dW/dr at |r| and the unit vector e = r / |r|.
@@ -606,8 +654,8 @@ __device__ __forceinline__ void pair_force_add(const PairParams<T, DIM>& pp,
   }
 }
 
-// One (i, j) pair.  tj: the neighbour's particle type.
-template <typename T, int DIM, typename Rec>
+// One (i, j) pair.  tj: the neighbour's particle type.  WRAP: see min_image.
+template <typename T, int DIM, bool WRAP, typename Rec>
 __device__ __forceinline__ void pair_term(const BoxParams& p, const PairParams<T, DIM>& pp,
                                           const CollView& cv, const PairOwn<T, DIM>& o,
                                           const Rec& rj, int tj, PairAcc<T, DIM>& acc) {
@@ -617,7 +665,7 @@ __device__ __forceinline__ void pair_term(const BoxParams& p, const PairParams<T
   const bool pair_force = o.do_force && (o.fluid || fluid_j);
   if (!pair_grad && !pair_force) return;
   T r[3];
-  const T r2 = pair_sep<T, DIM>(pp, p.wall, o, rj, r);
+  const T r2 = pair_sep<T, DIM, WRAP>(pp, p.wall, o, rj, r);
   if (!(r2 < pp.rcutsq)) return;
   const T vj[3] = {(T)rj.vx, (T)rj.vy, (T)rec_vz<DIM>(rj)};
   T v[3];
@@ -674,7 +722,7 @@ __device__ __forceinline__ void pair_term(const BoxParams& p, const PairParams<T
 // computed before either is added, so that their dependency chains overlap, and the sums
 // take them in list order.  va, vb: the position holds a partner; an absent position is
 // computed from whatever its staging slot holds and not added.
-template <typename T, int DIM, typename Rec>
+template <typename T, int DIM, bool WRAP, typename Rec>
 __device__ __forceinline__ void pair_fluid_x2(const BoxParams& p, const PairParams<T, DIM>& pp,
                                               const PairOwn<T, DIM>& o, const Rec& ra, bool va,
                                               const Rec& rb, bool vb, PairAcc<T, DIM>& acc) {
@@ -685,7 +733,7 @@ __device__ __forceinline__ void pair_fluid_x2(const BoxParams& p, const PairPara
   const bool valid[2] = {va, vb};
 #pragma unroll
   for (int u = 0; u < 2; ++u) {
-    const T r2 = pair_sep<T, DIM>(pp, p.wall, o, *rj[u], r[u]);
+    const T r2 = pair_sep<T, DIM, WRAP>(pp, p.wall, o, *rj[u], r[u]);
     in[u] = valid[u] && r2 < pp.rcutsq;
     v[u][0] = o.v[0] - (T)rj[u]->vx;
     v[u][1] = o.v[1] - (T)rj[u]->vy;

@@ -37,6 +37,13 @@ enum ErrInfo : int {
   kErrStepLo = 2,    // device step counter (completed steps) at the first report, low word
   kErrStepHi = 3,    // ... high word
   kErrPhase = 4,     // FailPhase of the first report
+  // nonzero when a position may lie outside [0, L] along a periodic axis: cleared before
+  // the hash of each search and set by the hash for every position it finds outside, by the
+  // half-kicks for every position they leave outside, and by any write of positions from
+  // the host.  While it is set the list build places every candidate by its minimum image;
+  // while it is clear the pair passes may drop the minimum image for particles clear of the
+  // periodic faces (clear_of_faces).
+  kPosOutside = 5,
   kErrInfoLen = 8,
 };
 

@@ -63,6 +63,7 @@ __global__ void k_vv1_particles(Dev d) {
   if (xi > p.L[0]) xi = xi - p.L[0];
   if (p.wall == 0 && yi > p.L[1]) yi = yi - p.L[1];
   if (p.dim == 3 && zi > p.L[2]) zi = zi - p.L[2];
+  if (outside_periodic(p, xi, yi, zi)) mark_outside(d);  // moved more than a box length
   x.x = xi;
   x.y = yi;
   x.z = zi;
@@ -207,6 +208,7 @@ __global__ void k_vv1_colloids(Dev d) {
       if (x.z < 0) x.z = x.z + p.L[2];
       if (x.z > p.L[2]) x.z = x.z - p.L[2];
     }
+    if (outside_periodic(p, x.x, x.y, x.z)) mark_outside(d);
     d.pos[slot] = x;
   }
 }
@@ -241,6 +243,7 @@ __global__ void k_hash(Dev d) {
   int ti = d.tinfo[i];
   const BoxParams& p = d.box[box_of(ti)];
   double4 x = d.pos[i];
+  if (outside_periodic(p, x.x, x.y, x.z)) mark_outside(d);  // cleared before this pass
   int c = hash_cell(p, x.x, x.y, x.z);
   if (c < 0) {
     raise_status(d, c == -2 ? kStatNaN : kStatCellRange, d.gid[i], kPhaseHash);
@@ -289,14 +292,14 @@ __global__ void k_reorder(Dev d) {
 
 // Density contribution of one list entry (kernel_densities.cu:52-163 with kernel_W.cu):
 // the exact distance test, then W(r) with r from one reciprocal square root; the
-// particle itself (r2 = 0) contributes W(0).
-template <typename T, int DIM>
+// particle itself (r2 = 0) contributes W(0).  WRAP: see min_image.
+template <typename T, int DIM, bool WRAP = true>
 __device__ __forceinline__ T density_term(const typename V4<T>::type& xi,
                                           const typename V4<T>::type& xj, const T L[3],
                                           const T h[3], int wall, T rcutsq, T rcut_inv, T cw) {
   T rx = xi.x - xj.x, ry = xi.y - xj.y, rz = DIM == 3 ? xi.z - xj.z : T(0);
-  min_image<T, DIM>(rx, ry, rz, L, h, wall);
-  const T r2 = DIM == 3 ? rx * rx + ry * ry + rz * rz : rx * rx + ry * ry;
+  min_image<T, DIM, WRAP>(rx, ry, rz, L, h, wall);
+  const T r2 = norm2(rx, ry, rz, DIM == 3);
   if (!(r2 < rcutsq)) return T(0);
   const T r = r2 > T(0) ? r2 * rsqrt(r2) : T(0);
   return sph_w<T>(r, rcut_inv, cw);
@@ -390,6 +393,63 @@ __device__ __forceinline__ unsigned list_test2(unsigned hits, f32x2 xi, f32x2 yi
   return __funnelshift_l(hi, hits, 1);
 }
 
+// Candidate placement.  A candidate of a neighbour cell's range is staged with that cell's
+// periodic shift, except in two cases where it must be placed at its minimum image about the
+// centre of the listing cell:
+//  - a stale range: an emptied cell keeps the range of the search that last saw it occupied
+//    (kernel_cell_ranges.cu:13-33); after the sort those slots hold whatever particles, from
+//    anywhere in the box, and the consumers take them by the minimum image as the reference
+//    does (kernel_densities.cu:90-110), so some are neighbours through another face;
+//  - a position outside the box (err_info[kPosOutside]): the hash's linear cell index runs
+//    on into the next row, so a particle can sit in a range far from its position.
+// With at least 3 cells per axis (cell >= rcut) the image about the centre is the one within
+// the cutoff of every particle of the cell, if any is.  A warp with a stale neighbour range,
+// or every warp while a position is outside, places all its candidates so; the others keep
+// the per-cell shift, which needs no test per candidate.
+//
+// v: a candidate's unshifted offset from the cell's corner along one axis; c the cell's
+// width, L the box's.
+__device__ __forceinline__ float stale_offset(float v, double c, double L) {
+  const float r = v - (float)(0.5 * c), hl = (float)(0.5 * L);
+  return r > hl ? v - (float)L : (r < -hl ? v + (float)L : v);
+}
+// The same with the bounds precomputed (lo = c/2 - L/2, hi = c/2 + L/2; an axis that does
+// not wrap has infinite bounds).
+__device__ __forceinline__ float frame_offset(float v, const float* lo, const float* hi,
+                                              const float* L, int q) {
+  v = v > hi[q] ? v - L[q] : v;
+  return v < lo[q] ? v + L[q] : v;
+}
+
+// Neighbour cell q (0 .. 3^d - 1, x slowest) of cell (cx, cy, cz) of box p with the
+// periodic wrap; false where the row does not exist (beyond a wall).
+template <int DIM>
+__device__ __forceinline__ bool neighbour_cell(const BoxParams& p, int cx, int cy, int cz,
+                                               int q, int& nc) {
+  constexpr int kNZ = DIM == 3 ? 3 : 1;
+  const int N0 = p.Ncells[0], N1 = p.Ncells[1], N2 = p.Ncells[2];
+  int nx = cx + q / (3 * kNZ) - 1, ny = cy + (q / kNZ) % 3 - 1;
+  int nz = DIM == 3 ? cz + q % 3 - 1 : 0;
+  if (nx < 0) nx += N0;
+  if (nx >= N0) nx -= N0;
+  if (DIM == 3) {
+    if (nz < 0) nz += N2;
+    if (nz >= N2) nz -= N2;
+  }
+  if (!p.wall) {
+    if (ny < 0) ny += N1;
+    if (ny >= N1) ny -= N1;
+  }
+  if (ny < 0 || ny >= N1) return false;
+  nc = p.cell0 + (DIM == 3 ? (nz * N1 + ny) * N0 + nx : ny * N0 + nx);
+  return true;
+}
+
+// An emptied cell whose reference range still lists slots.
+__device__ __forceinline__ bool stale_cell(const Dev& d, int nc) {
+  return d.cell_end[nc] >= d.cell_start[nc] && d.cell_begin[nc] == d.cell_begin[nc + 1];
+}
+
 template <int DIM, int TPC>
 __global__ void __launch_bounds__(kListWarps * 32) k_build_lists(Dev d) {
   static_assert(TPC == 32 || TPC == 16, "a warp or a half-warp per cell");
@@ -397,8 +457,15 @@ __global__ void __launch_bounds__(kListWarps * 32) k_build_lists(Dev d) {
   __shared__ __align__(16) float stage_x[kListWarps][32];
   __shared__ __align__(16) float stage_y[kListWarps][32];
   __shared__ __align__(16) float stage_z[kListWarps][32];
+  __shared__ float frame[kListWarps][2][9];  // per group: lo[3], hi[3], L[3] (frame_offset)
   const int w = threadIdx.x >> 5, lane = threadIdx.x & 31;
   if (step_aborted_warp(d)) return;
+  // a position outside the box (the hash's flag) may be sorted into a cell other than its
+  // own (the linear cell index runs on into the next row): then every candidate is placed
+  // by its minimum image, as in a stale range
+  int out_flag = 0;
+  if (lane == 0) out_flag = *(volatile const int*)(d.err_info + kPosOutside);
+  const bool any_out = __shfl_sync(SPH_FULL, out_flag, 0) != 0;
   const int sub = lane / TPC, gl = lane % TPC;  // group within the warp, lane within the group
   float* stx = &stage_x[w][sub * TPC];
   float* sty = &stage_y[w][sub * TPC];
@@ -433,194 +500,210 @@ __global__ void __launch_bounds__(kListWarps * 32) k_build_lists(Dev d) {
   // by shuffle; a half-warp group loads them as it goes
   constexpr int kNZ = DIM == 3 ? 3 : 1;
   int rs = 0, re = -1;
+  bool found = false;  // a stale neighbour range
   if (TPC == 32 && live && lane < 9 * kNZ) {
-    const int ddx = lane / (3 * kNZ) - 1, ddy = (lane / kNZ) % 3 - 1;
-    const int ddz = DIM == 3 ? lane % 3 - 1 : 0;
-    int nx = cx + ddx, ny = cy + ddy, nz = cz + ddz;
-    if (nx < 0) nx += N0;
-    if (nx >= N0) nx -= N0;
-    if (DIM == 3) {
-      if (nz < 0) nz += N2;
-      if (nz >= N2) nz -= N2;
-    }
-    if (!p.wall) {
-      if (ny < 0) ny += N1;
-      if (ny >= N1) ny -= N1;
-    }
-    if (ny >= 0 && ny < N1) {
-      const int nc = p.cell0 + (DIM == 3 ? (nz * N1 + ny) * N0 + nx : ny * N0 + nx);
+    int nc;
+    if (neighbour_cell<DIM>(p, cx, cy, cz, lane, nc)) {
       rs = d.cell_start[nc] + p.slot0;
       re = d.cell_end[nc] + p.slot0;
+      found = stale_cell(d, nc);
     }
   }
-  for (int t0 = 0; t0 < span; t0 += TPC) {
-    const int i = beg + t0 + gl;
-    const bool active = i < end;
-    float xi = 0.f, yi = 0.f, zi = 0.f;
-    bool odd = false, lost = false;
-    if (active) {
-      const double4 x = ld_pos<DIM>(d.pos + i);
-      xi = (float)(x.x - ox);
-      yi = (float)(x.y - oy);
-      zi = (float)(x.z - oz);
-      int ax = 0, ay = 0, az = 0;
-      if (own_cell(p, x.x, x.y, x.z, ax, ay, az)) {
-        odd = (ax != cx) || (ay != cy) || (DIM == 3 && az != cz);
-      } else {
-        // not finite or far outside the box: already reported by the hash; no neighbours
-        lost = true;
-        const bool finite = isfinite(x.x) && isfinite(x.y) && isfinite(x.z);
-        raise_status(d, finite ? kStatCellRange : kStatNaN, d.gid[i], kPhaseLists);
-      }
+  if (TPC == 16 && live) {
+    for (int q = gl; q < 9 * kNZ; q += TPC) {
+      int nc;
+      if (neighbour_cell<DIM>(p, cx, cy, cz, q, nc)) found = found || stale_cell(d, nc);
     }
-    const bool listed = active && !odd && !lost;
-    const f32x2 xi2 = f2_pack(xi, xi), yi2 = f2_pack(yi, yi), zi2 = f2_pack(zi, zi);
-    const f32x2 ncut22 = f2_pack(-cut2, -cut2);
-    int2* col = d.nchunk + (listed ? i : 0);  // this particle's chunks, stride Npad
-    int cnt = 0;                              // this lane's candidates
-    int kc = 0;                               // this lane's chunks with hits
-    for (int ddx = -1; ddx <= 1; ++ddx)
-      for (int ddy = -1; ddy <= 1; ++ddy)
-        for (int ddz = (DIM == 3 ? -1 : 0); ddz <= (DIM == 3 ? 1 : 0); ++ddz) {
-          int nx = cx + ddx, ny = cy + ddy, nz = cz + ddz;
-          double sx = 0.0, sy = 0.0, sz = 0.0;
-          if (nx < 0) { nx += N0; sx = -p.L[0]; }
-          if (nx >= N0) { nx -= N0; sx = p.L[0]; }
-          if (DIM == 3) {
-            if (nz < 0) { nz += N2; sz = -p.L[2]; }
-            if (nz >= N2) { nz -= N2; sz = p.L[2]; }
-          }
-          if (!p.wall) {
-            if (ny < 0) { ny += N1; sy = -p.L[1]; }
-            if (ny >= N1) { ny -= N1; sy = p.L[1]; }
-          }
-          // an empty range where the neighbour row does not exist (walls) or the group idles
-          int s = 0, e = -1;
-          if (TPC == 32) {
-            const int q = ((ddx + 1) * 3 + (ddy + 1)) * kNZ + (DIM == 3 ? ddz + 1 : 0);
-            s = __shfl_sync(SPH_FULL, rs, q);
-            e = __shfl_sync(SPH_FULL, re, q);
-          } else if (live && ny >= 0 && ny < N1) {
-            const int nc = p.cell0 + (DIM == 3 ? (nz * N1 + ny) * N0 + nx : ny * N0 + nx);
-            s = d.cell_start[nc] + p.slot0;
-            e = d.cell_end[nc] + p.slot0;
-          }
-          const int nch = e >= s ? (e - s + TPC) / TPC : 0;
-          const int nchw = TPC == 32 ? nch : warp_max(nch);
-          for (int k = 0; k < nchw; ++k) {
-            const int c0 = s + k * TPC;
-            const int j = c0 + gl;
-            float vx = 1e30f, vy = 1e30f, vz = 1e30f;  // padding: never a hit
-            if (k < nch && j <= e) {
-              const double4 xj = ld_pos<DIM>(d.pos + j);
-              vx = (float)(xj.x + sx - ox);
-              vy = (float)(xj.y + sy - oy);
-              vz = (float)(xj.z + sz - oz);
-            }
-            stx[gl] = vx;
-            sty[gl] = vy;
-            if (DIM == 3) stz[gl] = vz;
-            __syncwarp();
-            const int n = k < nch ? min(TPC, e - c0 + 1) : 0;
-            // hit mask of this chunk; staged candidate q is slot c0 + q.  A half-warp group
-            // runs a fixed trip count, which keeps both halves on one instruction stream.
-            const int m = TPC == 32 ? (n + 3) & ~3 : TPC;
-            unsigned hits = 0u;
-            if (TPC == 16 || listed) {
-#pragma unroll 1
-              for (int q = 0; q < m; q += 4) {
-                const ulonglong2 cx4 = *reinterpret_cast<const ulonglong2*>(stx + q);
-                const ulonglong2 cy4 = *reinterpret_cast<const ulonglong2*>(sty + q);
-                const ulonglong2 cz4 = DIM == 3 ? *reinterpret_cast<const ulonglong2*>(stz + q)
-                                                : make_ulonglong2(0ull, 0ull);
-                hits = list_test2<DIM>(hits, xi2, yi2, zi2, ncut22, cx4.x, cy4.x, cz4.x);
-                hits = list_test2<DIM>(hits, xi2, yi2, zi2, ncut22, cx4.y, cy4.y, cz4.y);
-              }
-              // first candidate was shifted in first: align it to bit 31 (bit 31 - q is
-              // candidate q, the consumers' order of leading zeros)
-              hits = m > 0 ? hits << (32 - m) : 0u;
-              if (TPC == 16) hits &= (listed && n > 0) ? ~(0xFFFFFFFFu >> n) : 0u;
-            }
-            if (hits != 0u) {  // a chunk with hits: (first slot, mask) in the next entry
-              if (kc < cap) col[(size_t)kc * Np] = make_int2(c0, (int)hits);
-              cnt += __popc(hits);
-              ++kc;
-            }
-            __syncwarp();  // the stage is refilled by the next chunk
-          }
+  }
+  // minimum-image placement for the whole warp (see stale_offset)
+  const bool mi = any_out || __any_sync(SPH_FULL, found);
+  if (mi && gl == 0) {
+    float* f = frame[w][sub];
+    for (int q = 0; q < 3; ++q) {
+      const bool wraps = q == 0 || (q == 1 && !p.wall) || (q == 2 && DIM == 3);
+      const float c = (float)(0.5 * p.cell_size[q]), h = (float)(0.5 * p.L[q]);
+      f[q] = wraps ? c - h : -3.0e38f;
+      f[3 + q] = wraps ? c + h : 3.0e38f;
+      f[6 + q] = (float)p.L[q];
+    }
+  }
+  __syncwarp();
+  const float* flo = frame[w][sub];
+  const float* fhi = flo + 3;
+  const float* fL = flo + 6;
+  // the particle loop, in the cheap form (per-cell shifts) or the minimum-image one
+  auto walk = [&](auto mi_tag) {
+    constexpr bool kMI = decltype(mi_tag)::value;
+    for (int t0 = 0; t0 < span; t0 += TPC) {
+      const int i = beg + t0 + gl;
+      const bool active = i < end;
+      float xi = 0.f, yi = 0.f, zi = 0.f;
+      bool odd = false, lost = false;
+      if (active) {
+        const double4 x = ld_pos<DIM>(d.pos + i);
+        xi = (float)(x.x - ox);
+        yi = (float)(x.y - oy);
+        zi = (float)(x.z - oz);
+        int ax = 0, ay = 0, az = 0;
+        if (own_cell(p, x.x, x.y, x.z, ax, ay, az)) {
+          odd = (ax != cx) || (ay != cy) || (DIM == 3 && az != cz);
+        } else {
+          // not finite or far outside the box: already reported by the hash; no neighbours
+          lost = true;
+          const bool finite = isfinite(x.x) && isfinite(x.y) && isfinite(x.z);
+          raise_status(d, finite ? kStatCellRange : kStatNaN, d.gid[i], kPhaseLists);
         }
-    if (active && !odd) {
-      d.nbr_cnt[i] = cnt;
-      d.nbr_nch[i] = min(kc, cap);
-    }
-    maxch = max(maxch, kc);
-    // particles exactly on the upper box edge: their own neighbour cells, the whole warp
-    // testing one such particle's candidates at a time
-    unsigned odd_mask = __ballot_sync(SPH_FULL, active && odd);
-    while (odd_mask) {
-      const int l = __ffs(odd_mask) - 1;
-      odd_mask &= odd_mask - 1;
-      // the particle and its cell's geometry, from the lane that holds it
-      const int ti = __shfl_sync(SPH_FULL, i, l);
-      const int tb = __shfl_sync(SPH_FULL, b, l);
-      const BoxParams& tp = d.box[tb];
-      const double4 xt = d.pos[ti];
-      int ax = 0, ay = 0, az = 0;
-      own_cell(tp, xt.x, xt.y, xt.z, ax, ay, az);  // checked above: cannot fail
-      const int M0 = tp.Ncells[0], M1 = tp.Ncells[1], M2 = tp.Ncells[2];
-      const double tox = ax * tp.cell_size[0];
-      const double toy = ay * tp.cell_size[1] - (tp.wall ? tp.wall_width : 0.0);
-      const double toz = DIM == 3 ? az * tp.cell_size[2] : 0.0;
-      const float tcut2 = (float)tp.list_cut2;
-      const float txi = (float)(xt.x - tox), tyi = (float)(xt.y - toy), tzi = (float)(xt.z - toz);
-      int tcnt = 0, tk = 0;
+      }
+      const bool listed = active && !odd && !lost;
+      const f32x2 xi2 = f2_pack(xi, xi), yi2 = f2_pack(yi, yi), zi2 = f2_pack(zi, zi);
+      const f32x2 ncut22 = f2_pack(-cut2, -cut2);
+      int2* col = d.nchunk + (listed ? i : 0);  // this particle's chunks, stride Npad
+      int cnt = 0;                              // this lane's candidates
+      int kc = 0;                               // this lane's chunks with hits
       for (int ddx = -1; ddx <= 1; ++ddx)
         for (int ddy = -1; ddy <= 1; ++ddy)
           for (int ddz = (DIM == 3 ? -1 : 0); ddz <= (DIM == 3 ? 1 : 0); ++ddz) {
-            int nx = ax + ddx, ny = ay + ddy, nz = az + ddz;
+            int nx = cx + ddx, ny = cy + ddy, nz = cz + ddz;
             double sx = 0.0, sy = 0.0, sz = 0.0;
-            if (nx < 0) { nx += M0; sx = -tp.L[0]; }
-            if (nx >= M0) { nx -= M0; sx = tp.L[0]; }
+            if (nx < 0) { nx += N0; sx = -p.L[0]; }
+            if (nx >= N0) { nx -= N0; sx = p.L[0]; }
             if (DIM == 3) {
-              if (nz < 0) { nz += M2; sz = -tp.L[2]; }
-              if (nz >= M2) { nz -= M2; sz = tp.L[2]; }
+              if (nz < 0) { nz += N2; sz = -p.L[2]; }
+              if (nz >= N2) { nz -= N2; sz = p.L[2]; }
             }
-            if (!tp.wall) {
-              if (ny < 0) { ny += M1; sy = -tp.L[1]; }
-              if (ny >= M1) { ny -= M1; sy = tp.L[1]; }
+            if (!p.wall) {
+              if (ny < 0) { ny += N1; sy = -p.L[1]; }
+              if (ny >= N1) { ny -= N1; sy = p.L[1]; }
             }
-            if (ny < 0 || ny >= M1) continue;
-            const int nc = tp.cell0 + (DIM == 3 ? (nz * M1 + ny) * M0 + nx : ny * M0 + nx);
-            const int s = d.cell_start[nc] + tp.slot0, e = d.cell_end[nc] + tp.slot0;
-            for (int c0 = s; c0 <= e; c0 += 32) {
-              const int j = c0 + lane;
-              bool hit = false;
-              if (j <= e) {
-                double4 xj = d.pos[j];
-                const float rx = txi - (float)(xj.x + sx - tox);
-                const float ry = tyi - (float)(xj.y + sy - toy);
-                float r2 = rx * rx + ry * ry;
-                if (DIM == 3) {
-                  const float rz = tzi - (float)(xj.z + sz - toz);
-                  r2 += rz * rz;
+            // an empty range where the neighbour row does not exist (walls) or the group idles
+            int s = 0, e = -1;
+            if (TPC == 32) {
+              const int q = ((ddx + 1) * 3 + (ddy + 1)) * kNZ + (DIM == 3 ? ddz + 1 : 0);
+              s = __shfl_sync(SPH_FULL, rs, q);
+              e = __shfl_sync(SPH_FULL, re, q);
+            } else if (live && ny >= 0 && ny < N1) {
+              const int nc = p.cell0 + (DIM == 3 ? (nz * N1 + ny) * N0 + nx : ny * N0 + nx);
+              s = d.cell_start[nc] + p.slot0;
+              e = d.cell_end[nc] + p.slot0;
+            }
+            const int nch = e >= s ? (e - s + TPC) / TPC : 0;
+            const int nchw = TPC == 32 ? nch : warp_max(nch);
+            for (int k = 0; k < nchw; ++k) {
+              const int c0 = s + k * TPC;
+              const int j = c0 + gl;
+              float vx = 1e30f, vy = 1e30f, vz = 1e30f;  // padding: never a hit
+              if (k < nch && j <= e) {
+                const double4 xj = ld_pos<DIM>(d.pos + j);
+                if constexpr (kMI) {
+                  vx = frame_offset((float)(xj.x - ox), flo, fhi, fL, 0);
+                  vy = frame_offset((float)(xj.y - oy), flo, fhi, fL, 1);
+                  vz = frame_offset((float)(xj.z - oz), flo, fhi, fL, 2);
+                } else {
+                  vx = (float)(xj.x + sx - ox);
+                  vy = (float)(xj.y + sy - oy);
+                  vz = (float)(xj.z + sz - oz);
                 }
-                hit = r2 < tcut2;
               }
-              const unsigned hits = __brev(__ballot_sync(SPH_FULL, hit));
-              if (hits != 0u) {
-                if (lane == 0 && tk < cap) d.nchunk[(size_t)tk * Np + ti] = make_int2(c0, (int)hits);
-                tcnt += __popc(hits);
-                ++tk;
+              stx[gl] = vx;
+              sty[gl] = vy;
+              if (DIM == 3) stz[gl] = vz;
+              __syncwarp();
+              const int n = k < nch ? min(TPC, e - c0 + 1) : 0;
+              // hit mask of this chunk; staged candidate q is slot c0 + q.  A half-warp group
+              // runs a fixed trip count, which keeps both halves on one instruction stream.
+              const int m = TPC == 32 ? (n + 3) & ~3 : TPC;
+              unsigned hits = 0u;
+              if (TPC == 16 || listed) {
+  #pragma unroll 1
+                for (int q = 0; q < m; q += 4) {
+                  const ulonglong2 cx4 = *reinterpret_cast<const ulonglong2*>(stx + q);
+                  const ulonglong2 cy4 = *reinterpret_cast<const ulonglong2*>(sty + q);
+                  const ulonglong2 cz4 = DIM == 3 ? *reinterpret_cast<const ulonglong2*>(stz + q)
+                                                  : make_ulonglong2(0ull, 0ull);
+                  hits = list_test2<DIM>(hits, xi2, yi2, zi2, ncut22, cx4.x, cy4.x, cz4.x);
+                  hits = list_test2<DIM>(hits, xi2, yi2, zi2, ncut22, cx4.y, cy4.y, cz4.y);
+                }
+                // first candidate was shifted in first: align it to bit 31 (bit 31 - q is
+                // candidate q, the consumers' order of leading zeros)
+                hits = m > 0 ? hits << (32 - m) : 0u;
+                if (TPC == 16) hits &= (listed && n > 0) ? ~(0xFFFFFFFFu >> n) : 0u;
               }
+              if (hits != 0u) {  // a chunk with hits: (first slot, mask) in the next entry
+                if (kc < cap) col[(size_t)kc * Np] = make_int2(c0, (int)hits);
+                cnt += __popc(hits);
+                ++kc;
+              }
+              __syncwarp();  // the stage is refilled by the next chunk
             }
           }
-      if (lane == 0) {
-        d.nbr_cnt[ti] = tcnt;
-        d.nbr_nch[ti] = min(tk, cap);
+      if (active && !odd) {
+        d.nbr_cnt[i] = cnt;
+        d.nbr_nch[i] = min(kc, cap);
       }
-      maxch = max(maxch, tk);
+      maxch = max(maxch, kc);
+      // particles exactly on the upper box edge: their own neighbour cells, the whole warp
+      // testing one such particle's candidates at a time
+      unsigned odd_mask = __ballot_sync(SPH_FULL, active && odd);
+      while (odd_mask) {
+        const int l = __ffs(odd_mask) - 1;
+        odd_mask &= odd_mask - 1;
+        // the particle and its cell's geometry, from the lane that holds it
+        const int ti = __shfl_sync(SPH_FULL, i, l);
+        const int tb = __shfl_sync(SPH_FULL, b, l);
+        const BoxParams& tp = d.box[tb];
+        const double4 xt = d.pos[ti];
+        int ax = 0, ay = 0, az = 0;
+        own_cell(tp, xt.x, xt.y, xt.z, ax, ay, az);  // checked above: cannot fail
+        const double tox = ax * tp.cell_size[0];
+        const double toy = ay * tp.cell_size[1] - (tp.wall ? tp.wall_width : 0.0);
+        const double toz = DIM == 3 ? az * tp.cell_size[2] : 0.0;
+        const float tcut2 = (float)tp.list_cut2;
+        const float txi = (float)(xt.x - tox), tyi = (float)(xt.y - toy), tzi = (float)(xt.z - toz);
+        int tcnt = 0, tk = 0;
+        for (int q = 0; q < 9 * kNZ; ++q) {
+          int nc;
+          if (!neighbour_cell<DIM>(tp, ax, ay, az, q, nc)) continue;
+          const int s = d.cell_start[nc] + tp.slot0, e = d.cell_end[nc] + tp.slot0;
+          for (int c0 = s; c0 <= e; c0 += 32) {
+            const int j = c0 + lane;
+            bool hit = false;
+            if (j <= e) {
+              // rare: every candidate at its minimum image about the particle's own cell
+              double4 xj = d.pos[j];
+              const float vx = stale_offset((float)(xj.x - tox), tp.cell_size[0], tp.L[0]);
+              float vy = (float)(xj.y - toy);
+              if (!tp.wall) vy = stale_offset(vy, tp.cell_size[1], tp.L[1]);
+              float vz = (float)(xj.z - toz);
+              if (DIM == 3) vz = stale_offset(vz, tp.cell_size[2], tp.L[2]);
+              const float rx = txi - vx;
+              const float ry = tyi - vy;
+              float r2 = rx * rx + ry * ry;
+              if (DIM == 3) {
+                const float rz = tzi - vz;
+                r2 += rz * rz;
+              }
+              hit = r2 < tcut2;
+            }
+            const unsigned hits = __brev(__ballot_sync(SPH_FULL, hit));
+            if (hits != 0u) {
+              if (lane == 0 && tk < cap) d.nchunk[(size_t)tk * Np + ti] = make_int2(c0, (int)hits);
+              tcnt += __popc(hits);
+              ++tk;
+            }
+          }
+        }
+        if (lane == 0) {
+          d.nbr_cnt[ti] = tcnt;
+          d.nbr_nch[ti] = min(tk, cap);
+        }
+        maxch = max(maxch, tk);
+      }
     }
-  }
+  };
+  if (mi)
+    walk(std::true_type{});
+  else
+    walk(std::false_type{});
   // warp max of the chunk counts -> capacity check
   maxch = warp_max(maxch);
   if (lane == 0 && maxch > 0) {
@@ -675,16 +758,16 @@ __global__ void k_colloid_cells(Dev d, int nboxes) {
   }
 }
 
-template <typename T, int DIM>
-__global__ void k_density(Dev d) {
+// One lane's density sum over its list, in list order.  The positions of kAhead entries are
+// loaded before they are summed (each term depends on a gathered position: with one load in
+// flight per lane the pass waited on memory, 5 long-scoreboard stalls per instruction).
+// Measured at 128^3 (FP64, with the plain separations): 1.16 ms with one entry at a time,
+// 1.10 ms with two, 1.21 and 1.22 ms with three and four (registers, fewer warps).
+template <typename T, int DIM, bool WRAP>
+__device__ __forceinline__ double density_sum(const Dev& d, const typename V4<T>::type* P,
+                                              int i, const BoxParams& p) {
   using V = typename V4<T>::type;
-  const int i = blockIdx.x * blockDim.x + threadIdx.x;
-  if (i >= d.Ntot) return;
-  if (step_aborted(d)) return;
-  // positions: the double state itself, or its float copy in mixed precision
-  const V* __restrict__ P = sizeof(T) == 8 ? reinterpret_cast<const V*>(d.pos)
-                                           : reinterpret_cast<const V*>(d.pos_f);
-  const BoxParams& p = d.box[box_of(d.tinfo[i])];
+  constexpr int kAhead = 2;
   const T L[3] = {(T)p.L[0], (T)p.L[1], (T)p.L[2]};
   const T h[3] = {(T)p.halfL[0], (T)p.halfL[1], (T)p.halfL[2]};
   const T rcutsq = (T)p.rcutsq;
@@ -694,16 +777,47 @@ __global__ void k_density(Dev d) {
   NbrIter it;
   it.init(d, i);
   T dens = T(0), comp = T(0);  // comp: Kahan compensation of a float sum
-  for (int k = 0; k < n; ++k) {
-    const int j = it.next();
-    if (j < 0) break;
-    const T w = density_term<T, DIM>(xi, ld_pos<DIM>(P + j), L, h, p.wall, rcutsq, rcut_inv, cw);
-    if constexpr (Compensated<T>::on)
-      kahan_add(dens, comp, w);
-    else
-      dens = dens + w;
+  for (int k = 0; k < n; k += kAhead) {
+    int j[kAhead];
+    V x[kAhead];
+#pragma unroll
+    for (int u = 0; u < kAhead; ++u) j[u] = k + u < n ? it.next() : -1;
+#pragma unroll
+    for (int u = 0; u < kAhead; ++u) x[u] = ld_pos<DIM>(P + (j[u] >= 0 ? j[u] : i));
+#pragma unroll
+    for (int u = 0; u < kAhead; ++u) {
+      if (j[u] < 0) break;
+      const T w = density_term<T, DIM, WRAP>(xi, x[u], L, h, p.wall, rcutsq, rcut_inv, cw);
+      if constexpr (Compensated<T>::on)
+        kahan_add(dens, comp, w);
+      else
+        dens = dens + w;
+    }
   }
-  density_epilogue<T, DIM>(d, i, p, (double)dens - (double)comp);
+  return (double)dens - (double)comp;
+}
+
+// Whole warps (lanes past the end mirror the last slot and store nothing), so that a warp
+// of particles clear of the periodic faces takes the sums without the minimum image.
+template <typename T, int DIM>
+__global__ void k_density(Dev d) {
+  using V = typename V4<T>::type;
+  const int i0 = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i0 - (int)(threadIdx.x & 31) >= d.Ntot) return;  // whole warps only
+  if (step_aborted_warp(d)) return;
+  const bool active = i0 < d.Ntot;
+  const int i = active ? i0 : d.Ntot - 1;
+  // positions: the double state itself, or its float copy in mixed precision
+  const V* __restrict__ P = sizeof(T) == 8 ? reinterpret_cast<const V*>(d.pos)
+                                           : reinterpret_cast<const V*>(d.pos_f);
+  const BoxParams& p = d.box[box_of(d.tinfo[i])];
+  const V xi = ld_pos<DIM>(P + i);
+  double dens;
+  if (warp_plain_image(d, clear_of_faces<T, DIM>(p, xi.x, xi.y, xi.z)))
+    dens = density_sum<T, DIM, false>(d, P, i, p);
+  else
+    dens = density_sum<T, DIM, true>(d, P, i, p);
+  if (active) density_epilogue<T, DIM>(d, i, p, dens);
 }
 
 // Density over neighbour-cell tiles: one warp per cell, as the list build.  The positions
@@ -981,7 +1095,8 @@ struct PairWalk {
 };
 
 // One position per step: the copies for position k + 1 are in flight while k is evaluated.
-template <typename T, int DIM>
+// WRAP: see min_image.
+template <typename T, int DIM, bool WRAP>
 __device__ __forceinline__ void pair_walk1(const PairWalk<T, DIM>& W, NbrIter& it,
                                            PairAcc<T, DIM>& acc) {
   using Rec = typename RecFor<T, DIM>::type;
@@ -1005,7 +1120,7 @@ __device__ __forceinline__ void pair_walk1(const PairWalk<T, DIM>& W, NbrIter& i
       const StagedRec<T, Rec> R(W.sb + (k & 1) * St::kRows + lane * St::kStride);
       int tj;
       if constexpr (DIM == 3) tj = type_of(R.r.tinfo); else tj = type_of(tc);
-      pair_term<T, DIM>(W.p, W.pp, W.cv, W.o, R.r, tj, acc);
+      pair_term<T, DIM, WRAP>(W.p, W.pp, W.cv, W.o, R.r, tj, acc);
     }
     __syncwarp();  // buffer k & 1 is refilled at position k + 2
     jc = jn;
@@ -1015,7 +1130,7 @@ __device__ __forceinline__ void pair_walk1(const PairWalk<T, DIM>& W, NbrIter& i
 
 // Two positions per step: the copies for positions k + 2, k + 3 are in flight while k and
 // k + 1 are evaluated, side by side where every lane's partners there are fluid.
-template <typename T, int DIM>
+template <typename T, int DIM, bool WRAP>
 __device__ __forceinline__ void pair_walk2(const PairWalk<T, DIM>& W, NbrIter& it,
                                            PairAcc<T, DIM>& acc) {
   using Rec = typename RecFor<T, DIM>::type;
@@ -1056,10 +1171,10 @@ __device__ __forceinline__ void pair_walk2(const PairWalk<T, DIM>& W, NbrIter& i
     // side by side only where every lane of the warp qualifies: a warp split between the
     // two forms would run both
     if (__all_sync(SPH_FULL, W.o.fluid && (!va || tja == 0) && (!vb || tjb == 0))) {
-      pair_fluid_x2<T, DIM>(W.p, W.pp, W.o, A.r, va, B.r, vb, acc);
+      pair_fluid_x2<T, DIM, WRAP>(W.p, W.pp, W.o, A.r, va, B.r, vb, acc);
     } else {
-      if (va) pair_term<T, DIM>(W.p, W.pp, W.cv, W.o, A.r, tja, acc);
-      if (vb) pair_term<T, DIM>(W.p, W.pp, W.cv, W.o, B.r, tjb, acc);
+      if (va) pair_term<T, DIM, WRAP>(W.p, W.pp, W.cv, W.o, A.r, tja, acc);
+      if (vb) pair_term<T, DIM, WRAP>(W.p, W.pp, W.cv, W.o, B.r, tjb, acc);
     }
     __syncwarp();  // this position pair's buffers are refilled at position k + 4
     ja = jna;
@@ -1102,10 +1217,25 @@ __global__ void __launch_bounds__(PairShape<T, DIM>::kWarps * 32, PairShape<T, D
   NbrIter it;
   it.init(d, is);
   const PairWalk<T, DIM> W{d, rec, &stage[w][0][0], lane, i, n, nmax, p, pp, cv, o};
-  if constexpr (Sh::kILP == 2)
-    pair_walk2<T, DIM>(W, it, acc);
-  else
-    pair_walk1<T, DIM>(W, it, acc);
+  auto walk = [&](auto wrap_tag) {
+    constexpr bool kWrap = decltype(wrap_tag)::value;
+    if constexpr (Sh::kILP == 2)
+      pair_walk2<T, DIM, kWrap>(W, it, acc);
+    else
+      pair_walk1<T, DIM, kWrap>(W, it, acc);
+  };
+  // Warps clear of the periodic faces drop the minimum image, in 3D only: a second copy of
+  // the 2D two-position walk cost the 512-box ensemble's pair pass more in instruction
+  // fetch (3.62 -> 5.05 ms, its small boxes mix both kinds of warp on every SM) than the
+  // shorter separations saved; the 3D passes gain 5 %.
+  if constexpr (DIM == 3) {
+    if (warp_plain_image(d, clear_of_faces<T, DIM>(p, o.x, o.y, o.z)))
+      walk(std::false_type{});
+    else
+      walk(std::true_type{});
+  } else {
+    walk(std::true_type{});
+  }
   if (active) pair_store<T, DIM, MODE, EXT>(d, i, p, o, acc);
 }
 
@@ -1575,6 +1705,7 @@ __global__ void k_scatter_field(Dev d, int f, const double* in) {
     double4 x = d.pos[s];
     if (comp == 0) x.x = v; else if (comp == 1) x.y = v; else if (comp == 2) x.z = v; else x.w = v;
     d.pos[s] = x;
+    mark_outside(d);  // until the next search has looked at the new positions
   } else if (iv) {
     double4 u = d.vel[s];
     if (comp == 0) u.x = v; else if (comp == 1) u.y = v; else u.z = v;
@@ -1631,6 +1762,8 @@ int launch_vv2(const Launch& L, bool particles) {
 }
 
 int launch_hash(const Launch& L) {
+  // the hash sets the flag again for every position it finds outside the box
+  if (cudaMemsetAsync(L.d.err_info + kPosOutside, 0, sizeof(int), S(L)) != cudaSuccess) return 1;
   k_hash<<<blocks(L.d.Ntot, kT), kT, 0, S(L)>>>(L.d);
   return check(L);
 }
