@@ -853,6 +853,27 @@ sph_status sph_create_ensemble(int nboxes, const sph_input* inputs,
       ok = false;
   };
   up((void*)d.box, params.data(), params.size() * sizeof(BoxParams));
+  d.one_box = nboxes == 1 ? 1 : 0;
+  if (nboxes == 1) {
+    const BoxParams& q = params[0];
+    PairConsts& k = d.pc;
+    for (int a = 0; a < 3; ++a) {
+      k.L[a] = q.L[a];
+      k.h[a] = q.halfL[a];
+      k.Lf[a] = (float)q.L[a];
+      k.hf[a] = (float)q.halfL[a];
+    }
+    k.rcutsq = q.rcutsq;
+    k.rcut_inv = q.rcut_inv;
+    k.c_gradw = q.c_gradw;
+    k.a = q.a;
+    k.b = q.b;
+    k.rcutsqf = (float)q.rcutsq;
+    k.rcut_invf = (float)q.rcut_inv;
+    k.c_gradwf = (float)q.c_gradw;
+    k.af = (float)q.a;
+    k.bf = (float)q.b;
+  }
   if (full) {
     up(d.pos, pos.data(), Np * sizeof(double4));
     up(d.vel, vel.data(), Np * sizeof(double4));

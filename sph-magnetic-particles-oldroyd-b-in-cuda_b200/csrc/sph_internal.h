@@ -151,6 +151,14 @@ struct alignas(16) RecF2 {
 };
 static_assert(sizeof(RecF2) == 32, "RecF2 layout");
 
+// The pair constants of a context with one box, in both precisions: kernels receive Dev by
+// value, so these live in the constant bank, where the pair pass's arithmetic reads them as
+// operands instead of holding them in registers (PairParams has the same layout).
+struct PairConsts {
+  double L[3], h[3], rcutsq, rcut_inv, c_gradw, a, b;
+  float Lf[3], hf[3], rcutsqf, rcut_invf, c_gradwf, af, bf;
+};
+
 // Device pointers, passed to kernels by value.
 struct Dev {
   int Ntot, Npad, nboxes, Ctot, ncoll, nwallseg;
@@ -219,6 +227,8 @@ struct Dev {
   int* err_info;       // kErrInfoLen ints, see ErrInfo
   int grad_all;        // fused pair pass: velocity gradient of every particle, not only fluid
   int fold_vv2;        // fused pair pass: also the step's second half-kick of fluid particles
+  int one_box;         // a single box: its pair constants are in pc
+  PairConsts pc;
 };
 
 // Colloid state layout in Dev::cs (each row ncoll long).

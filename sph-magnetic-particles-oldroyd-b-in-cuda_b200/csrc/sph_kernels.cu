@@ -1000,17 +1000,36 @@ __global__ void k_pressure(Dev d) {
 //  - kWarps: warps per block; kMinBlocks: resident blocks per SM the register allocation
 //    is held to (FP64 3D: 168 registers, which its working set fits without spilling; the
 //    two-position passes 128; the float 2D pass needs 96).
+//  - One-box 3D contexts (k_pairs<..., ONE = true>) read the pair constants from the
+//    constant bank (Dev::pc) instead of registers: 128^3 pair pass 3.59 -> 3.55 ms (FP64)
+//    and 2.43 -> 2.38 ms (mixed) at the same shape.  The FP64 3D pass then fits 128
+//    registers with 32 bytes of spill, but at 16 warps per SM (4 blocks of 4 warps or 8 of
+//    2) it took 4.03 and 3.98 ms: the larger shared-memory carve-out leaves L1 too little
+//    for the record gathers.
 template <typename T, int DIM>
 struct PairShape {
   using Rec = typename RecFor<T, DIM>::type;
   static constexpr bool kF64 = sizeof(T) == 8;
   static constexpr bool kF2D = !kF64 && DIM == 2;
-  static constexpr int kILP = (kF64 && DIM == 3) || kF2D ? 1 : 2;
+  static constexpr bool kF64_3D = kF64 && DIM == 3;
+  static constexpr int kILP = kF64_3D || kF2D ? 1 : 2;
   // the float 2D pass runs 2-warp blocks (measured 2.29 vs 2.35 ms on the 512-box ensemble;
   // the float 3D pass was slower with them, the FP64 passes unchanged)
   static constexpr int kWarps = kF2D ? 2 : 4;
   static constexpr int kMinBlocks = kF2D ? 6 : (kILP == 1 ? 3 : 4);
 };
+
+// The pair constants of a one-box context, viewed as PairParams (same layout).
+template <typename T, int DIM>
+__device__ __forceinline__ const PairParams<T, DIM>& one_box_params(const Dev& d) {
+  static_assert(sizeof(PairParams<double, DIM>) == 11 * sizeof(double) &&
+                    sizeof(PairParams<float, DIM>) == 11 * sizeof(float),
+                "PairParams layout");
+  if constexpr (sizeof(T) == 8)
+    return *reinterpret_cast<const PairParams<T, DIM>*>(d.pc.L);
+  else
+    return *reinterpret_cast<const PairParams<T, DIM>*>(d.pc.Lf);
+}
 
 template <typename Rec>
 struct PairStage {
@@ -1184,9 +1203,10 @@ __device__ __forceinline__ void pair_walk2(const PairWalk<T, DIM>& W, NbrIter& i
   }
 }
 
-template <typename T, int DIM, int MODE, bool EXT>
-__global__ void __launch_bounds__(PairShape<T, DIM>::kWarps * 32, PairShape<T, DIM>::kMinBlocks)
-    k_pairs(Dev d) {
+template <typename T, int DIM, int MODE, bool EXT, bool ONE>
+__global__ void __launch_bounds__(PairShape<T, DIM>::kWarps * 32,
+                                  PairShape<T, DIM>::kMinBlocks)
+    k_pairs(const __grid_constant__ Dev d) {
   using Sh = PairShape<T, DIM>;
   using Rec = typename Sh::Rec;
   using St = PairStage<Rec>;
@@ -1203,8 +1223,9 @@ __global__ void __launch_bounds__(PairShape<T, DIM>::kWarps * 32, PairShape<T, D
   const Rec* __restrict__ rec = reinterpret_cast<const Rec*>(d.rec);
   const int ti = d.tinfo[is];
   const BoxParams& p = d.box[box_of(ti)];
-  PairParams<T, DIM> pp;
-  pp.load(p);
+  PairParams<T, DIM> ppl;
+  if constexpr (!ONE) ppl.load(p);
+  const PairParams<T, DIM>& pp = ONE ? one_box_params<T, DIM>(d) : ppl;
   const CollView cv{d.cs, d.ncoll};
   PairOwn<T, DIM> o;
   load_own<T, DIM, MODE>(d, is, ti, rec[is], o);
@@ -1835,18 +1856,27 @@ int launch_pressure(const Launch& L) {
   return check(L);
 }
 
-template <typename T, int DIM>
-static void pairs_dispatch(const Launch& L, int mode, int with_ext) {
+template <typename T, int DIM, bool ONE>
+static void pairs_launch(const Launch& L, int mode, int with_ext) {
   constexpr int nt = PairShape<T, DIM>::kWarps * 32;
   const int nb = blocks(L.d.Ntot, nt);
   if (mode == kPairGradvAll)
-    k_pairs<T, DIM, kPairGradvAll, false><<<nb, nt, 0, S(L)>>>(L.d);
+    k_pairs<T, DIM, kPairGradvAll, false, ONE><<<nb, nt, 0, S(L)>>>(L.d);
   else if (mode == kPairForcesOnly)
-    k_pairs<T, DIM, kPairForcesOnly, false><<<nb, nt, 0, S(L)>>>(L.d);
+    k_pairs<T, DIM, kPairForcesOnly, false, ONE><<<nb, nt, 0, S(L)>>>(L.d);
   else if (with_ext)
-    k_pairs<T, DIM, kPairFused, true><<<nb, nt, 0, S(L)>>>(L.d);
+    k_pairs<T, DIM, kPairFused, true, ONE><<<nb, nt, 0, S(L)>>>(L.d);
   else
-    k_pairs<T, DIM, kPairFused, false><<<nb, nt, 0, S(L)>>>(L.d);
+    k_pairs<T, DIM, kPairFused, false, ONE><<<nb, nt, 0, S(L)>>>(L.d);
+}
+
+// One-box 3D contexts take the constant-bank form; 2D ones are mostly ensembles.
+template <typename T, int DIM>
+static void pairs_dispatch(const Launch& L, int mode, int with_ext) {
+  if (DIM == 3 && L.d.one_box)
+    pairs_launch<T, DIM, DIM == 3>(L, mode, with_ext);
+  else
+    pairs_launch<T, DIM, false>(L, mode, with_ext);
 }
 
 int launch_pairs_dim(const Launch& L, int dim, int mode, int with_ext) {
