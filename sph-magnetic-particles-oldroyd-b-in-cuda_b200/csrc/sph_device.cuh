@@ -717,6 +717,28 @@ __device__ __forceinline__ void pair_term(const BoxParams& p, const PairParams<T
   }
 }
 
+// One list position of a fluid particle whose partner there is a fluid particle (or is
+// absent: valid false): pair_term's fluid-fluid term without its type tests, for warps whose
+// every lane has such a position (fewer branches, longer blocks for the scheduler).
+template <typename T, int DIM, bool WRAP, typename Rec>
+__device__ __forceinline__ void pair_fluid_x1(const BoxParams& p, const PairParams<T, DIM>& pp,
+                                              const PairOwn<T, DIM>& o, const Rec& rj,
+                                              bool valid, PairAcc<T, DIM>& acc) {
+  T r[3];
+  const T r2 = pair_sep<T, DIM, WRAP>(pp, p.wall, o, rj, r);
+  if (!(valid && r2 < pp.rcutsq)) return;
+  const T v[3] = {o.v[0] - (T)rj.vx, o.v[1] - (T)rj.vy, o.v[2] - (T)rec_vz<DIM>(rj)};
+  PairRadial<T, DIM> g;
+  g.eval(pp, r2, r);
+  if (o.do_grad) pair_grad_add<T, DIM>(o, g, v, acc);
+  if (o.do_force) {
+    T Pj[6];
+#pragma unroll
+    for (int q = 0; q < 6; ++q) Pj[q] = rec_P<DIM>(rj, q);
+    pair_force_add<T, DIM>(pp, g, v, o.P, Pj, o.invd, (T)rj.invd, acc);
+  }
+}
+
 // Two list positions of a fluid particle whose partners there are fluid particles (or
 // absent), evaluated side by side.  Each term is pair_term's fluid-fluid term; both are
 // computed before either is added, so that their dependency chains overlap, and the sums

@@ -1135,12 +1135,16 @@ __device__ __forceinline__ void pair_walk1(const PairWalk<T, DIM>& W, NbrIter& i
     cp_async_commit();
     cp_async_wait_prev();  // position k has landed (this lane's copies) ...
     __syncwarp();          // ... and every other lane's
-    if (jc >= 0 && jc != W.i) {
-      const StagedRec<T, Rec> R(W.sb + (k & 1) * St::kRows + lane * St::kStride);
-      int tj;
-      if constexpr (DIM == 3) tj = type_of(R.r.tinfo); else tj = type_of(tc);
+    const bool valid = jc >= 0 && jc != W.i;
+    const StagedRec<T, Rec> R(W.sb + (k & 1) * St::kRows + lane * St::kStride);
+    int tj;
+    if constexpr (DIM == 3) tj = type_of(R.r.tinfo); else tj = type_of(tc);
+    // the fluid-fluid form where every lane of the warp qualifies (a warp split between the
+    // forms would run both)
+    if (__all_sync(SPH_FULL, W.o.fluid && (!valid || tj == 0)))
+      pair_fluid_x1<T, DIM, WRAP>(W.p, W.pp, W.o, R.r, valid, acc);
+    else if (valid)
       pair_term<T, DIM, WRAP>(W.p, W.pp, W.cv, W.o, R.r, tj, acc);
-    }
     __syncwarp();  // buffer k & 1 is refilled at position k + 2
     jc = jn;
     tc = tn;
