@@ -412,8 +412,8 @@ def run_ours(args, world, rank, local, dist, wl):
 
 
 def mixed_summary(args, local, wl, steps=10, cmp_steps=5):
-    """The same workload in mixed precision (pair sums in float with compensated
-    accumulation, state in FP64): device time per step, and its deviation from the FP64
+    """The same workload in mixed precision (pair terms in float, summed in FP64, state in
+    FP64): device time per step, and its deviation from the FP64
     engine after cmp_steps steps from the same start (max |mixed - fp64| / group scale)."""
     import sph_b200
 

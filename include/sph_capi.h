@@ -50,8 +50,9 @@ typedef enum sph_status {
 
 typedef enum sph_precision {
   SPH_PREC_FP64 = 0,  /* all arithmetic in double, as the reference's default build     */
-  SPH_PREC_MIXED = 1  /* pair arithmetic in float; positions, velocities, conformation
-                         tensor, integration and global reductions in double            */
+  SPH_PREC_MIXED = 1  /* pair arithmetic in float, its per-particle sums in double;
+                         positions, velocities, conformation tensor, integration and
+                         global reductions in double                                    */
 } sph_precision;
 
 /* The keys of the reference's `input` file (src/system_read_input.cpp:102-269,

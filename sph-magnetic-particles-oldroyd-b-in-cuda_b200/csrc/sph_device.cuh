@@ -5,6 +5,8 @@
 #include <cuda_runtime.h>
 #include <math.h>
 
+#include <type_traits>
+
 #include "sph_internal.h"
 
 namespace sph {
@@ -488,18 +490,25 @@ struct PairOwn {
   bool fluid, do_grad, do_force;
 };
 
-// Compensated summation of the float pair sums (density, velocity gradient, forces) in
-// mixed precision; FP64 sums stay plain.
-#ifndef SPH_FLOAT_SUMS_COMPENSATED
-#define SPH_FLOAT_SUMS_COMPENSATED 1
-#endif
+// Sums of the float pair terms in mixed precision (density, velocity gradient, forces):
+// kind 1 compensated float sums (Kahan), kind 2 FP64 accumulators of the float terms (kept:
+// more accurate, and at 128^3 the pair pass 2.41 -> 2.39 ms and the density 0.74 -> 0.73 ms,
+// the conversions and FP64 adds running on the otherwise idle FP64 pipe).  FP64 sums stay
+// plain.  S: the accumulator type.
+constexpr int kFloatSums = 2;
 template <typename T>
-struct Compensated {
-  static constexpr bool on = false;
+struct SumKind {
+  static constexpr int kind = 0;
+  using S = T;
 };
 template <>
-struct Compensated<float> {
-  static constexpr bool on = SPH_FLOAT_SUMS_COMPENSATED != 0;
+struct SumKind<float> {
+  static constexpr int kind = kFloatSums;
+  using S = std::conditional_t<kFloatSums == 2, double, float>;
+};
+template <typename T>
+struct Compensated {
+  static constexpr bool on = SumKind<T>::kind == 1;
 };
 
 // Kahan step: s + c tracks the exact sum of the terms to about one rounding of s.
@@ -512,20 +521,32 @@ __device__ __forceinline__ void kahan_add(float& s, float& c, float x) {
 
 template <typename T, int DIM>
 struct PairAcc {
-  // float sums (mixed precision) are compensated: each carries its rounding error in a
-  // second float (Kahan), added back when the sum is stored
+  // float sums (mixed precision) are compensated, each carrying its rounding error in a
+  // second float (Kahan) added back when the sum is stored, or FP64 (SumKind)
+  using S = typename SumKind<T>::S;
   static constexpr bool kComp = Compensated<T>::on;
-  T g[DIM][DIM];
-  T f[3];
+  static constexpr bool kTermwise = SumKind<T>::kind != 0;  // a pair's force as one term
+  S g[DIM][DIM];
+  S f[3];
   T cg[DIM][DIM];
   T cf[3];
   __device__ __forceinline__ void zero() {
 #pragma unroll
     for (int a = 0; a < DIM; ++a)
 #pragma unroll
-      for (int c = 0; c < DIM; ++c) g[a][c] = cg[a][c] = T(0);
-    f[0] = f[1] = f[2] = T(0);
+      for (int c = 0; c < DIM; ++c) {
+        g[a][c] = S(0);
+        cg[a][c] = T(0);
+      }
+    f[0] = f[1] = f[2] = S(0);
     cf[0] = cf[1] = cf[2] = T(0);
+  }
+  // s (with compensation c) += x
+  __device__ __forceinline__ static void add(S& s, T& c, T x) {
+    if constexpr (kComp)
+      kahan_add(s, c, x);
+    else
+      s += (S)x;
   }
   __device__ __forceinline__ double grad(int a, int c) const {
     return kComp ? (double)g[a][c] - (double)cg[a][c] : (double)g[a][c];
@@ -593,8 +614,8 @@ __device__ __forceinline__ void pair_grad_add(const PairOwn<T, DIM>& o, const Pa
     const T se = s * g.e[a];
 #pragma unroll
     for (int c = 0; c < DIM; ++c) {
-      if constexpr (PairAcc<T, DIM>::kComp)
-        kahan_add(acc.g[a][c], acc.cg[a][c], se * v[c]);
+      if constexpr (PairAcc<T, DIM>::kTermwise)
+        PairAcc<T, DIM>::add(acc.g[a][c], acc.cg[a][c], se * v[c]);
       else
         acc.g[a][c] += se * v[c];
     }
@@ -613,8 +634,8 @@ __device__ __forceinline__ void pair_force_add(const PairParams<T, DIM>& pp,
   const T* e = g.e;
   const T aux = gw * di * dj * g.rinv;
   const T aux1 = pp.a * aux;
-  if constexpr (PairAcc<T, DIM>::kComp) {
-    // the pair's force as one term per component, then one compensated add
+  if constexpr (PairAcc<T, DIM>::kTermwise) {
+    // the pair's force as one term per component, then one compensated (or FP64) add
     const T axx = -gw * (Pi[0] + Pj[0]);
     const T axy = -gw * (Pi[1] + Pj[1]);
     const T ayy = -gw * (Pi[2] + Pj[2]);
@@ -630,9 +651,9 @@ __device__ __forceinline__ void pair_force_add(const PairParams<T, DIM>& pp,
       t2 = axz * e[0] + ayz * e[1] + azz * e[2];
     }
     const T aux2 = pp.b * aux * ev;
-    kahan_add(acc.f[0], acc.cf[0], t0 + (aux1 * v[0] + aux2 * e[0]));
-    kahan_add(acc.f[1], acc.cf[1], t1 + (aux1 * v[1] + aux2 * e[1]));
-    if (DIM == 3) kahan_add(acc.f[2], acc.cf[2], t2 + (aux1 * v[2] + aux2 * e[2]));
+    PairAcc<T, DIM>::add(acc.f[0], acc.cf[0], t0 + (aux1 * v[0] + aux2 * e[0]));
+    PairAcc<T, DIM>::add(acc.f[1], acc.cf[1], t1 + (aux1 * v[1] + aux2 * e[1]));
+    if (DIM == 3) PairAcc<T, DIM>::add(acc.f[2], acc.cf[2], t2 + (aux1 * v[2] + aux2 * e[2]));
   } else {
     // -gw (Pi + Pj).e and the viscous terms folded into the sums by fused multiply-adds
     const T ngw = -gw;
@@ -719,8 +740,14 @@ __device__ __forceinline__ void pair_term(const BoxParams& p, const PairParams<T
 
 // One list position of a fluid particle whose partner there is a fluid particle (or is
 // absent: valid false): pair_term's fluid-fluid term without its type tests, for warps whose
-// every lane has such a position (fewer branches, longer blocks for the scheduler).
-template <typename T, int DIM, bool WRAP, typename Rec>
+// every lane has such a position (fewer branches, longer blocks for the scheduler).  For a
+// fluid particle the terms taken follow from MODE alone (load_own's do_grad, do_force).
+template <int MODE>
+struct FluidTerms {
+  static constexpr bool kGrad = MODE != kPairForcesOnly;
+  static constexpr bool kForce = MODE != kPairGradvAll;
+};
+template <typename T, int DIM, bool WRAP, int MODE, typename Rec>
 __device__ __forceinline__ void pair_fluid_x1(const BoxParams& p, const PairParams<T, DIM>& pp,
                                               const PairOwn<T, DIM>& o, const Rec& rj,
                                               bool valid, PairAcc<T, DIM>& acc) {
@@ -730,8 +757,8 @@ __device__ __forceinline__ void pair_fluid_x1(const BoxParams& p, const PairPara
   const T v[3] = {o.v[0] - (T)rj.vx, o.v[1] - (T)rj.vy, o.v[2] - (T)rec_vz<DIM>(rj)};
   PairRadial<T, DIM> g;
   g.eval(pp, r2, r);
-  if (o.do_grad) pair_grad_add<T, DIM>(o, g, v, acc);
-  if (o.do_force) {
+  if constexpr (FluidTerms<MODE>::kGrad) pair_grad_add<T, DIM>(o, g, v, acc);
+  if constexpr (FluidTerms<MODE>::kForce) {
     T Pj[6];
 #pragma unroll
     for (int q = 0; q < 6; ++q) Pj[q] = rec_P<DIM>(rj, q);
@@ -744,7 +771,7 @@ __device__ __forceinline__ void pair_fluid_x1(const BoxParams& p, const PairPara
 // computed before either is added, so that their dependency chains overlap, and the sums
 // take them in list order.  va, vb: the position holds a partner; an absent position is
 // computed from whatever its staging slot holds and not added.
-template <typename T, int DIM, bool WRAP, typename Rec>
+template <typename T, int DIM, bool WRAP, int MODE, typename Rec>
 __device__ __forceinline__ void pair_fluid_x2(const BoxParams& p, const PairParams<T, DIM>& pp,
                                               const PairOwn<T, DIM>& o, const Rec& ra, bool va,
                                               const Rec& rb, bool vb, PairAcc<T, DIM>& acc) {
@@ -765,8 +792,8 @@ __device__ __forceinline__ void pair_fluid_x2(const BoxParams& p, const PairPara
 #pragma unroll
   for (int u = 0; u < 2; ++u) {
     if (!in[u]) continue;
-    if (o.do_grad) pair_grad_add<T, DIM>(o, g[u], v[u], acc);
-    if (o.do_force) {
+    if constexpr (FluidTerms<MODE>::kGrad) pair_grad_add<T, DIM>(o, g[u], v[u], acc);
+    if constexpr (FluidTerms<MODE>::kForce) {
       T Pj[6];
 #pragma unroll
       for (int q = 0; q < 6; ++q) Pj[q] = rec_P<DIM>(*rj[u], q);

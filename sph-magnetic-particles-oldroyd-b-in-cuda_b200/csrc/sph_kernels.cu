@@ -776,7 +776,8 @@ __device__ __forceinline__ double density_sum(const Dev& d, const typename V4<T>
   const int n = d.nbr_cnt[i];
   NbrIter it;
   it.init(d, i);
-  T dens = T(0), comp = T(0);  // comp: Kahan compensation of a float sum
+  typename SumKind<T>::S dens = 0;
+  T comp = T(0);  // Kahan compensation of a float sum
   for (int k = 0; k < n; k += kAhead) {
     int j[kAhead];
     V x[kAhead];
@@ -889,7 +890,8 @@ __global__ void __launch_bounds__(kDensWarps * 32) k_density_cells(Dev d) {
     it.init(d, active ? i : beg);
     // the next list entry not yet summed (-1: none left)
     int jn = n > 0 ? it.next() : -1;
-    T dens = T(0), comp = T(0);  // comp: Kahan compensation of a float sum
+    typename SumKind<T>::S dens = 0;
+  T comp = T(0);  // Kahan compensation of a float sum
     auto add = [&](const V& xj) {
       const T wv = density_term<T, DIM>(xi, xj, L, h, p.wall, rcutsq, rcut_inv, cw);
       if constexpr (Compensated<T>::on)
@@ -1115,7 +1117,7 @@ struct PairWalk {
 
 // One position per step: the copies for position k + 1 are in flight while k is evaluated.
 // WRAP: see min_image.
-template <typename T, int DIM, bool WRAP>
+template <typename T, int DIM, bool WRAP, int MODE>
 __device__ __forceinline__ void pair_walk1(const PairWalk<T, DIM>& W, NbrIter& it,
                                            PairAcc<T, DIM>& acc) {
   using Rec = typename RecFor<T, DIM>::type;
@@ -1142,7 +1144,7 @@ __device__ __forceinline__ void pair_walk1(const PairWalk<T, DIM>& W, NbrIter& i
     // the fluid-fluid form where every lane of the warp qualifies (a warp split between the
     // forms would run both)
     if (__all_sync(SPH_FULL, W.o.fluid && (!valid || tj == 0)))
-      pair_fluid_x1<T, DIM, WRAP>(W.p, W.pp, W.o, R.r, valid, acc);
+      pair_fluid_x1<T, DIM, WRAP, MODE>(W.p, W.pp, W.o, R.r, valid, acc);
     else if (valid)
       pair_term<T, DIM, WRAP>(W.p, W.pp, W.cv, W.o, R.r, tj, acc);
     __syncwarp();  // buffer k & 1 is refilled at position k + 2
@@ -1153,7 +1155,7 @@ __device__ __forceinline__ void pair_walk1(const PairWalk<T, DIM>& W, NbrIter& i
 
 // Two positions per step: the copies for positions k + 2, k + 3 are in flight while k and
 // k + 1 are evaluated, side by side where every lane's partners there are fluid.
-template <typename T, int DIM, bool WRAP>
+template <typename T, int DIM, bool WRAP, int MODE>
 __device__ __forceinline__ void pair_walk2(const PairWalk<T, DIM>& W, NbrIter& it,
                                            PairAcc<T, DIM>& acc) {
   using Rec = typename RecFor<T, DIM>::type;
@@ -1194,7 +1196,7 @@ __device__ __forceinline__ void pair_walk2(const PairWalk<T, DIM>& W, NbrIter& i
     // side by side only where every lane of the warp qualifies: a warp split between the
     // two forms would run both
     if (__all_sync(SPH_FULL, W.o.fluid && (!va || tja == 0) && (!vb || tjb == 0))) {
-      pair_fluid_x2<T, DIM, WRAP>(W.p, W.pp, W.o, A.r, va, B.r, vb, acc);
+      pair_fluid_x2<T, DIM, WRAP, MODE>(W.p, W.pp, W.o, A.r, va, B.r, vb, acc);
     } else {
       if (va) pair_term<T, DIM, WRAP>(W.p, W.pp, W.cv, W.o, A.r, tja, acc);
       if (vb) pair_term<T, DIM, WRAP>(W.p, W.pp, W.cv, W.o, B.r, tjb, acc);
@@ -1245,9 +1247,9 @@ __global__ void __launch_bounds__(PairShape<T, DIM>::kWarps * 32,
   auto walk = [&](auto wrap_tag) {
     constexpr bool kWrap = decltype(wrap_tag)::value;
     if constexpr (Sh::kILP == 2)
-      pair_walk2<T, DIM, kWrap>(W, it, acc);
+      pair_walk2<T, DIM, kWrap, MODE>(W, it, acc);
     else
-      pair_walk1<T, DIM, kWrap>(W, it, acc);
+      pair_walk1<T, DIM, kWrap, MODE>(W, it, acc);
   };
   // Warps clear of the periodic faces drop the minimum image, in 3D only: a second copy of
   // the 2D two-position walk cost the 512-box ensemble's pair pass more in instruction
