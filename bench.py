@@ -80,7 +80,7 @@ B_ALG_PAIRS = {"fp64": (6 + 6 + 1 + 1 + 6 + 1 + 3 + 6) * 8 + 4,
 # by ncu on the 96^3 case of this workload (same lattice, same neighbours per particle):
 # DADD + DMUL + 2 DFMA thread instructions (each per-cycle rate times the SM sub-partition's
 # elapsed cycles) / particles (profiles/k_pairs_couette96_fp64.md).
-FP64_PAIR_FLOP = 11618.0
+FP64_PAIR_FLOP = 11626.9
 # FP64 peak of the B200: 148 SMs x 64 FP64 FMA lanes (ncu's dfma peak_sustained, 9,472 per
 # cycle) x 2 FLOP x the SM clock.
 FP64_LANES = 9472
