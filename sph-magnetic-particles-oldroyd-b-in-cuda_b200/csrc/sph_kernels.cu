@@ -997,11 +997,13 @@ __global__ void k_pressure(Dev d) {
 //
 // Launch shape of the pair pass per precision and dimension, as measured on B200:
 //  - kILP: list positions evaluated per step.  Two side by side (pair_fluid_x2) hide the
-//    latency of the float 3D and FP64 2D terms; the FP64 3D pass, held to 12 warps per SM
-//    by its 168 registers, and the float 2D pass run faster one position at a time.
+//    latency of the FP64 2D terms; the FP64 3D pass, held to 12 warps per SM by its 168
+//    registers, and the float passes run faster one position at a time (the float 3D pass
+//    since the one-position walk has its fluid-fluid form: 128^3 2.41 -> 2.38 ms, 96^3
+//    suspension 1.33 -> 1.28 ms; with 5 blocks per SM, 96 registers and spills, 2.51 ms).
 //  - kWarps: warps per block; kMinBlocks: resident blocks per SM the register allocation
 //    is held to (FP64 3D: 168 registers, which its working set fits without spilling; the
-//    two-position passes 128; the float 2D pass needs 96).
+//    FP64 2D two-position pass and the float 3D pass 128; the float 2D pass needs 96).
 //  - One-box 3D contexts (k_pairs<..., ONE = true>) read the pair constants from the
 //    constant bank (Dev::pc) instead of registers: 128^3 pair pass 3.59 -> 3.55 ms (FP64)
 //    and 2.43 -> 2.38 ms (mixed) at the same shape.  The FP64 3D pass then fits 128
@@ -1014,11 +1016,11 @@ struct PairShape {
   static constexpr bool kF64 = sizeof(T) == 8;
   static constexpr bool kF2D = !kF64 && DIM == 2;
   static constexpr bool kF64_3D = kF64 && DIM == 3;
-  static constexpr int kILP = kF64_3D || kF2D ? 1 : 2;
+  static constexpr int kILP = (kF64 && DIM == 2) ? 2 : 1;
   // the float 2D pass runs 2-warp blocks (measured 2.29 vs 2.35 ms on the 512-box ensemble;
   // the float 3D pass was slower with them, the FP64 passes unchanged)
   static constexpr int kWarps = kF2D ? 2 : 4;
-  static constexpr int kMinBlocks = kF2D ? 6 : (kILP == 1 ? 3 : 4);
+  static constexpr int kMinBlocks = kF2D ? 6 : (kF64_3D ? 3 : 4);
 };
 
 // The pair constants of a one-box context, viewed as PairParams (same layout).
