@@ -766,42 +766,6 @@ __device__ __forceinline__ void pair_fluid_x1(const BoxParams& p, const PairPara
   }
 }
 
-// Two list positions of a fluid particle whose partners there are fluid particles (or
-// absent), evaluated side by side.  Each term is pair_term's fluid-fluid term; both are
-// computed before either is added, so that their dependency chains overlap, and the sums
-// take them in list order.  va, vb: the position holds a partner; an absent position is
-// computed from whatever its staging slot holds and not added.
-template <typename T, int DIM, bool WRAP, int MODE, typename Rec>
-__device__ __forceinline__ void pair_fluid_x2(const BoxParams& p, const PairParams<T, DIM>& pp,
-                                              const PairOwn<T, DIM>& o, const Rec& ra, bool va,
-                                              const Rec& rb, bool vb, PairAcc<T, DIM>& acc) {
-  T r[2][3], v[2][3];
-  PairRadial<T, DIM> g[2];
-  bool in[2];
-  const Rec* rj[2] = {&ra, &rb};
-  const bool valid[2] = {va, vb};
-#pragma unroll
-  for (int u = 0; u < 2; ++u) {
-    const T r2 = pair_sep<T, DIM, WRAP>(pp, p.wall, o, *rj[u], r[u]);
-    in[u] = valid[u] && r2 < pp.rcutsq;
-    v[u][0] = o.v[0] - (T)rj[u]->vx;
-    v[u][1] = o.v[1] - (T)rj[u]->vy;
-    v[u][2] = o.v[2] - (T)rec_vz<DIM>(*rj[u]);
-    g[u].eval(pp, r2, r[u]);
-  }
-#pragma unroll
-  for (int u = 0; u < 2; ++u) {
-    if (!in[u]) continue;
-    if constexpr (FluidTerms<MODE>::kGrad) pair_grad_add<T, DIM>(o, g[u], v[u], acc);
-    if constexpr (FluidTerms<MODE>::kForce) {
-      T Pj[6];
-#pragma unroll
-      for (int q = 0; q < 6; ++q) Pj[q] = rec_P<DIM>(*rj[u], q);
-      pair_force_add<T, DIM>(pp, g[u], v[u], o.P, Pj, o.invd, (T)rj[u]->invd, acc);
-    }
-  }
-}
-
 // Second half-kick of a fluid particle's velocity, v += (dt / 2) f / m
 // (kernel_move_sys_VV_part2.cu:13-58), as explicit fused multiply-adds so that the step's
 // fused form and the standalone V_Verlet_step2 give the same bits.

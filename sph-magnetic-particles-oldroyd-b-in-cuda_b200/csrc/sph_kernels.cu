@@ -991,19 +991,18 @@ __global__ void k_pressure(Dev d) {
 // per instruction, that is 32 separate cache lines per instruction.  Instead the warp
 // copies the 32 records into shared memory cooperatively: kPieces consecutive lanes move
 // the pieces of one record, so one copy instruction covers whole lines of 32 / kPieces
-// records.  The copies for the next position (or the next two) are in flight (cp.async,
-// double buffer) while the current ones are evaluated.  Each lane then reads its records
+// records.  The copies for the next position are in flight (cp.async, double buffer)
+// while the current ones are evaluated.  Each lane then reads its records
 // from shared memory (row stride padded by one piece: conflict-free).
 //
-// Launch shape of the pair pass per precision and dimension, as measured on B200:
-//  - kILP: list positions evaluated per step.  Two side by side (pair_fluid_x2) hide the
-//    latency of the FP64 2D terms; the FP64 3D pass, held to 12 warps per SM by its 168
-//    registers, and the float passes run faster one position at a time (the float 3D pass
-//    since the one-position walk has its fluid-fluid form: 128^3 2.41 -> 2.38 ms, 96^3
-//    suspension 1.33 -> 1.28 ms; with 5 blocks per SM, 96 registers and spills, 2.51 ms).
+// Launch shape of the pair pass per precision and dimension, as measured on B200.  Every pass
+// evaluates one list position per step: with the fluid-fluid form of that walk, evaluating two
+// positions side by side (to overlap their dependency chains) measured slower everywhere
+// (float 3D at 128^3 2.41 vs 2.38 ms, FP64 2D on the 512-box ensemble 3.63 vs 3.52 ms).
 //  - kWarps: warps per block; kMinBlocks: resident blocks per SM the register allocation
-//    is held to (FP64 3D: 168 registers, which its working set fits without spilling; the
-//    FP64 2D two-position pass and the float 3D pass 128; the float 2D pass needs 96).
+//    is held to (FP64 3D: 168 registers, which its working set fits without spilling;
+//    float 3D 128; FP64 2D 96, with a few spills: 5 blocks 3.52 ms, 4 blocks 3.58 ms; the
+//    float 2D pass 80, in 2-warp blocks).
 //  - One-box 3D contexts (k_pairs<..., ONE = true>) read the pair constants from the
 //    constant bank (Dev::pc) instead of registers: 128^3 pair pass 3.59 -> 3.55 ms (FP64)
 //    and 2.43 -> 2.38 ms (mixed) at the same shape.  The FP64 3D pass then fits 128
@@ -1016,11 +1015,10 @@ struct PairShape {
   static constexpr bool kF64 = sizeof(T) == 8;
   static constexpr bool kF2D = !kF64 && DIM == 2;
   static constexpr bool kF64_3D = kF64 && DIM == 3;
-  static constexpr int kILP = (kF64 && DIM == 2) ? 2 : 1;
   // the float 2D pass runs 2-warp blocks (measured 2.29 vs 2.35 ms on the 512-box ensemble;
   // the float 3D pass was slower with them, the FP64 passes unchanged)
   static constexpr int kWarps = kF2D ? 2 : 4;
-  static constexpr int kMinBlocks = kF2D ? 6 : (kF64_3D ? 3 : 4);
+  static constexpr int kMinBlocks = kF2D ? 6 : (kF64_3D ? 3 : (kF64 ? 5 : 4));
 };
 
 // The pair constants of a one-box context, viewed as PairParams (same layout).
@@ -1117,10 +1115,10 @@ struct PairWalk {
   const PairOwn<T, DIM>& o;
 };
 
-// One position per step: the copies for position k + 1 are in flight while k is evaluated.
-// WRAP: see min_image.
+// A lane's walk over its list, one position per step: the copies for position k + 1 are in
+// flight while k is evaluated.  WRAP: see min_image.
 template <typename T, int DIM, bool WRAP, int MODE>
-__device__ __forceinline__ void pair_walk1(const PairWalk<T, DIM>& W, NbrIter& it,
+__device__ __forceinline__ void pair_walk(const PairWalk<T, DIM>& W, NbrIter& it,
                                            PairAcc<T, DIM>& acc) {
   using Rec = typename RecFor<T, DIM>::type;
   using St = PairStage<Rec>;
@@ -1155,62 +1153,6 @@ __device__ __forceinline__ void pair_walk1(const PairWalk<T, DIM>& W, NbrIter& i
   }
 }
 
-// Two positions per step: the copies for positions k + 2, k + 3 are in flight while k and
-// k + 1 are evaluated, side by side where every lane's partners there are fluid.
-template <typename T, int DIM, bool WRAP, int MODE>
-__device__ __forceinline__ void pair_walk2(const PairWalk<T, DIM>& W, NbrIter& it,
-                                           PairAcc<T, DIM>& acc) {
-  using Rec = typename RecFor<T, DIM>::type;
-  using St = PairStage<Rec>;
-  const int n = W.n, lane = W.lane;
-  int ja = n > 0 ? it.next() : -1;
-  int jb = n > 1 ? it.next() : -1;
-  int ta = DIM == 2 && ja >= 0 ? __ldg(&W.d.tinfo[ja]) : 0;
-  int tb = DIM == 2 && jb >= 0 ? __ldg(&W.d.tinfo[jb]) : 0;
-  stage_records<Rec>(W.sb, W.rec, ja, lane);
-  stage_records<Rec>(W.sb + St::kRows, W.rec, jb, lane);
-  cp_async_commit();
-  for (int k = 0; k < W.nmax; k += 2) {
-    const int k2 = k + 2;
-    const int jna = k2 < n ? it.next() : -1;
-    const int jnb = k2 + 1 < n ? it.next() : -1;
-    if (k2 < W.nmax) {
-      int4* nbuf = W.sb + ((k2 >> 1) & 1) * 2 * St::kRows;
-      stage_records<Rec>(nbuf, W.rec, jna, lane);
-      stage_records<Rec>(nbuf + St::kRows, W.rec, jnb, lane);
-    }
-    const int tna = DIM == 2 && jna >= 0 ? __ldg(&W.d.tinfo[jna]) : 0;
-    const int tnb = DIM == 2 && jnb >= 0 ? __ldg(&W.d.tinfo[jnb]) : 0;
-    cp_async_commit();
-    cp_async_wait_prev();  // positions k, k + 1 have landed (this lane's copies) ...
-    __syncwarp();          // ... and every other lane's
-    const int4* src = W.sb + ((k >> 1) & 1) * 2 * St::kRows + lane * St::kStride;
-    const StagedRec<T, Rec> A(src), B(src + St::kRows);
-    const bool va = ja >= 0 && ja != W.i, vb = jb >= 0 && jb != W.i;
-    int tja, tjb;
-    if constexpr (DIM == 3) {
-      tja = type_of(A.r.tinfo);
-      tjb = type_of(B.r.tinfo);
-    } else {
-      tja = type_of(ta);
-      tjb = type_of(tb);
-    }
-    // side by side only where every lane of the warp qualifies: a warp split between the
-    // two forms would run both
-    if (__all_sync(SPH_FULL, W.o.fluid && (!va || tja == 0) && (!vb || tjb == 0))) {
-      pair_fluid_x2<T, DIM, WRAP, MODE>(W.p, W.pp, W.o, A.r, va, B.r, vb, acc);
-    } else {
-      if (va) pair_term<T, DIM, WRAP>(W.p, W.pp, W.cv, W.o, A.r, tja, acc);
-      if (vb) pair_term<T, DIM, WRAP>(W.p, W.pp, W.cv, W.o, B.r, tjb, acc);
-    }
-    __syncwarp();  // this position pair's buffers are refilled at position k + 4
-    ja = jna;
-    jb = jnb;
-    ta = tna;
-    tb = tnb;
-  }
-}
-
 template <typename T, int DIM, int MODE, bool EXT, bool ONE>
 __global__ void __launch_bounds__(PairShape<T, DIM>::kWarps * 32,
                                   PairShape<T, DIM>::kMinBlocks)
@@ -1218,8 +1160,8 @@ __global__ void __launch_bounds__(PairShape<T, DIM>::kWarps * 32,
   using Sh = PairShape<T, DIM>;
   using Rec = typename Sh::Rec;
   using St = PairStage<Rec>;
-  // per warp: a double buffer of kILP staged positions
-  __shared__ int4 stage[Sh::kWarps][2 * Sh::kILP][St::kRows];
+  // per warp: a double buffer of staged positions
+  __shared__ int4 stage[Sh::kWarps][2][St::kRows];
   const int w = threadIdx.x >> 5, lane = threadIdx.x & 31;
   const int wbase = (blockIdx.x * Sh::kWarps + w) * 32;
   if (wbase >= d.Ntot) return;  // whole warps only: the lanes below cooperate
@@ -1247,16 +1189,12 @@ __global__ void __launch_bounds__(PairShape<T, DIM>::kWarps * 32,
   it.init(d, is);
   const PairWalk<T, DIM> W{d, rec, &stage[w][0][0], lane, i, n, nmax, p, pp, cv, o};
   auto walk = [&](auto wrap_tag) {
-    constexpr bool kWrap = decltype(wrap_tag)::value;
-    if constexpr (Sh::kILP == 2)
-      pair_walk2<T, DIM, kWrap, MODE>(W, it, acc);
-    else
-      pair_walk1<T, DIM, kWrap, MODE>(W, it, acc);
+    pair_walk<T, DIM, decltype(wrap_tag)::value, MODE>(W, it, acc);
   };
-  // Warps clear of the periodic faces drop the minimum image, in 3D only: a second copy of
-  // the 2D two-position walk cost the 512-box ensemble's pair pass more in instruction
-  // fetch (3.62 -> 5.05 ms, its small boxes mix both kinds of warp on every SM) than the
-  // shorter separations saved; the 3D passes gain 5 %.
+  // Warps clear of the periodic faces drop the minimum image, in 3D only: the 512-box 2D
+  // ensemble's small boxes put both kinds of warp on every SM, and the second copy of the
+  // walk cost more in instruction fetch than the shorter separations saved (FP64 2D pair
+  // pass 3.52 -> 3.54 ms, float 2D 2.23 -> 2.38 ms); the 3D passes gain 5 %.
   if constexpr (DIM == 3) {
     if (warp_plain_image(d, clear_of_faces<T, DIM>(p, o.x, o.y, o.z)))
       walk(std::false_type{});
