@@ -521,8 +521,9 @@ __device__ __forceinline__ void kahan_add(float& s, float& c, float x) {
 
 template <typename T, int DIM>
 struct PairAcc {
-  // float sums (mixed precision) are compensated, each carrying its rounding error in a
-  // second float (Kahan) added back when the sum is stored, or FP64 (SumKind)
+  // the sums of float pair terms (mixed precision) are FP64 accumulators, or, in the
+  // compensated form (SumKind kind 1), floats each carrying its rounding error in a second
+  // float (Kahan) that is added back when the sum is stored
   using S = typename SumKind<T>::S;
   static constexpr bool kComp = Compensated<T>::on;
   static constexpr bool kTermwise = SumKind<T>::kind != 0;  // a pair's force as one term
