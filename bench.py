@@ -344,9 +344,12 @@ def run_ours(args, world, rank, local, dist, wl):
         value = n * args.steps * world / (ms_max * 1e-3)
         # per-phase device times (CUDA events on the engine's stream), separate short pass
         phases = sysm.profile_phases(args.profile_steps)
-        # e2e: the reference's call sequence through the C ABI with host buffers
+        # e2e: the reference's call sequence through the C ABI with host buffers; the step's
+        # input (the magnetic moment) is copied from pinned host memory
+        import torch
+
+        m = torch.zeros(3, dtype=torch.float64).pin_memory().numpy()
         ke = []
-        m = np.zeros(3)
         e2e_steps = min(args.steps, args.e2e_steps)
         info = sysm.info()
         t0 = time.perf_counter()
