@@ -373,6 +373,39 @@ def test_step_graph_equals_method_sequence(name, precision, workdir):
     b.close()
 
 
+@pytest.mark.parametrize("precision", ["fp64", "mixed"])
+def test_3d_ensemble_equals_single_boxes(precision, workdir):
+    """3D boxes in one context against each box alone: a one-box context's pair pass reads
+    its constants from the constant bank, an ensemble's from each box's parameters; with
+    walls and without, warps clear of the periodic faces and not, the same bits."""
+    specs = [
+        dict(N=(24, 24, 24), L=(1.0, 1.0, 1.0), dim=3, overlap=3.0, wall=1, Vwall_top=0.2,
+             Vwall_bottom=-0.2, dt=2e-5, tau=0.5),
+        dict(N=(20, 16, 18), L=(1.25, 1.0, 1.125), dim=3, overlap=3.0, wall=0, ext_force_type=2,
+             ext_force=(1.0, 0.0, 0.0), dt=5e-5),
+    ]
+    paths = []
+    for k, s in enumerate(specs):
+        p = os.path.join(workdir, "input%d" % k)
+        sph_input.write_input(p, **s)
+        paths.append(p)
+    ens = sph_b200.System(paths, precision=precision)
+    ens.step(5)
+    ens.synchronize()
+    off = 0
+    for k, p in enumerate(paths):
+        one = sph_b200.System(p, precision=precision)
+        one.step(5)
+        one.synchronize()
+        n = one.N
+        for f in ["x", "y", "z", "vx", "vz", "fx", "fz", "dens", "cxy", "cyz"]:
+            assert np.array_equal(ens.field(f)[off:off + n], one.field(f)), (k, f)
+        assert np.array_equal(ens.wall_forces()[k], one.wall_forces()[0])
+        off += n
+        one.close()
+    ens.close()
+
+
 def test_ensemble_equals_single_boxes(workdir):
     """Boxes of different sizes and parameters in one context give, box by box, the same
     bits as each box run alone."""
